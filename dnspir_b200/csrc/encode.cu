@@ -1,0 +1,229 @@
+// encode.cu -- database encoding on the GPU (set_transformed_entries,
+// crates/pir/src/base_pir.rs:662-772).
+//
+// For a database of group order l with columns a_t (t < l, each a ring element
+// per lane), row c of the reference's transformed entries is
+//     E_c = lift_t( l^-1 * sigma_{5^-r}( A^_r ) ),   r = L-1-c,
+//     A^_r = sum_t a_t X^(-qbp 5^r t)          (main half)
+//     A~_r = sum_t a_t X^(+qbp 5^r t)          (conjugate half, l = N only)
+// (base_pir.rs STEP 3-6).  The reference reaches this with a column NTT, a
+// coset NTT per row, a Galois permutation per column, a reversal, and a lift
+// through the coefficient domain.  Here:
+//   cols: A_t = NTT_N(a_t)                                   (q1)
+//   rows: for each slot u, W_u = NTT_{N/qbp}(A_.[u]) (zero-padded over t);
+//         A^_r[u] and A~_r[u] are entries of W_u at the orbit of (2u+1) under 5
+//   lift: iNTT_N, centred lift, * l^-1 mod t, centred lift, NTT_N in q1 and q2.
+// The scan stores E_c permuted by the slot map it reads with, which cancels
+// sigma_{5^-r}: in the scan layout row c of the entries is NTT(lift(l^-1 A^_r))
+// in natural slot order.  The exactness argument is the reference's: every
+// coefficient of A^_r is below l * t < q1 / 2 in magnitude (:668-670).
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace dnspir {
+
+Group make_group(int log2n, uint32_t l) {
+  Group g;
+  g.log2n = log2n;
+  g.n = 1u << log2n;
+  g.l = l;
+  g.L = l < g.n ? l : g.n / 2;
+  g.H = l == g.n ? 2 : 1;
+  g.qbp = g.n / 2 / g.L;
+  return g;
+}
+
+namespace {
+
+__global__ void encode_cols_kernel(const uint16_t* __restrict__ in, uint32_t* __restrict__ A, int log2n,
+                                   uint32_t total, int ppc, NttTables T) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t n = 1u << log2n;
+  const uint32_t first = blockIdx.x * ppc;
+  const int cnt = min((uint32_t)ppc, total - first);
+  for (uint32_t b = threadIdx.x; b < (uint32_t)cnt * n; b += blockDim.x) sm[b] = in[(size_t)first * n + b];
+  __syncthreads();
+  ntt_fwd_smem(sm, log2n, cnt, T, 0);
+  for (uint32_t b = threadIdx.x; b < (uint32_t)cnt * n; b += blockDim.x) {
+    const uint32_t poly = b >> log2n, u = b & (n - 1);
+    A[(size_t)(first + poly) * n + u] = sm[(poly << log2n) + brv(u, log2n)];
+  }
+}
+
+// One block: U consecutive slots u of one lane.  Transforms the length-l
+// vector over t (zero-padded to n2 = N / qbp) and scatters the orbit values.
+__global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __restrict__ Ahat, Group g,
+                                   uint32_t l_in, int nl, int U, int logn2, const uint32_t* __restrict__ pow5,
+                                   NttTables T) {
+  extern __shared__ uint32_t sm[];
+  const int k = blockIdx.y;
+  const uint32_t u0 = blockIdx.x * U;
+  const uint32_t n2 = 1u << logn2;
+  const uint32_t N = g.n;
+  for (uint32_t b = threadIdx.x; b < (uint32_t)U * n2; b += blockDim.x) {
+    const uint32_t t = b / U, uu = b % U;
+    uint32_t v = 0;
+    if (t < l_in) v = A[((size_t)t * nl + k) * N + u0 + uu];
+    sm[uu * n2 + t] = v;
+  }
+  __syncthreads();
+  ntt_fwd_smem(sm, logn2, U, T, 0);
+  const uint32_t mask = 2 * n2 - 1;
+  const uint32_t outs = g.H * g.L * U;
+  for (uint32_t b = threadIdx.x; b < outs; b += blockDim.x) {
+    const uint32_t uu = b % U;
+    const uint32_t r = (b / U) % g.L;
+    const uint32_t h = b / (U * g.L);
+    const uint32_t u = u0 + uu;
+    const uint32_t g5 = ((2 * u + 1) * pow5[r]) & mask;
+    // slot s of W holds V(zeta^(-qbp (2s+1))): main needs exponent (2u+1) qbp 5^r
+    const uint32_t s = h == 0 ? ((mask + 1 - g5) & mask) >> 1 : g5 >> 1;
+    Ahat[(((size_t)h * g.L + r) * nl + k) * N + u] = sm[uu * n2 + brv(s, logn2)];
+  }
+}
+
+// One block: column r of half h for up to 8 lanes.
+__global__ void encode_lift_kernel(const uint32_t* __restrict__ Ahat, uint32_t* __restrict__ out, Group g, int nl,
+                                   int frame, uint32_t scale, const uint32_t* __restrict__ pow5inv, NttTables T) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t r = blockIdx.x, h = blockIdx.y;
+  const int lane0 = blockIdx.z * 8;
+  const int nlg = min(8, nl - lane0);
+  const uint32_t N = g.n;
+  const int logn = g.log2n;
+  uint32_t* x1 = sm;
+  uint32_t* x2 = sm + nlg * N;
+  for (uint32_t b = threadIdx.x; b < (uint32_t)nlg * N; b += blockDim.x) {
+    const uint32_t kk = b >> logn, u = b & (N - 1);
+    x1[(kk << logn) + brv(u, logn)] = Ahat[(((size_t)h * g.L + r) * nl + lane0 + kk) * N + u];
+  }
+  __syncthreads();
+  ntt_inv_smem(x1, logn, nlg, T, 0);
+  for (uint32_t b = threadIdx.x; b < (uint32_t)nlg * N; b += blockDim.x) {
+    const uint32_t v = x1[b];
+    const int32_t c = v > P1 / 2 ? (int32_t)v - (int32_t)P1 : (int32_t)v;
+    int32_t m = c % (int32_t)TPLAIN;
+    if (m < 0) m += TPLAIN;
+    m = (int32_t)(((uint32_t)m * scale) % TPLAIN);
+    const int32_t y = m > (int32_t)(TPLAIN / 2) ? m - (int32_t)TPLAIN : m;
+    x1[b] = y < 0 ? (uint32_t)(y + (int32_t)P1) : (uint32_t)y;
+    x2[b] = y < 0 ? (uint32_t)(y + (int32_t)P2) : (uint32_t)y;
+  }
+  __syncthreads();
+  ntt_fwd_smem2(sm, logn, nlg, nlg, T);
+  const uint32_t c = g.L - 1 - r;
+  if (frame == 0) {
+    // scan layout: 8 lanes interleaved, natural slot order
+    for (uint32_t b = threadIdx.x; b < 2 * N * SIMD; b += blockDim.x) {
+      const uint32_t p = b / (N * SIMD);
+      const uint32_t rem = b % (N * SIMD);
+      const uint32_t u = rem / SIMD, kk = rem % SIMD;
+      out[slab_off(g, p, h, c, 0, u) + kk] = sm[((p * nlg + kk) << logn) + brv(u, logn)];
+    }
+  } else {
+    // chain layout, bit-reversed positions, E_c[j] = E^_r[idx(5^-r (2j+1))]
+    const uint32_t mask = 2 * N - 1;
+    for (uint32_t b = threadIdx.x; b < 2 * (uint32_t)nlg * N; b += blockDim.x) {
+      const uint32_t p = b / (nlg * N);
+      const uint32_t rem = b % (nlg * N);
+      const uint32_t kk = rem >> logn, pos = rem & (N - 1);
+      const uint32_t j = brv(pos, logn);
+      const uint32_t src = gidx(pow5inv[r] * (2 * j + 1), mask);
+      out[((((size_t)p * g.H + h) * g.L + c) * nl + lane0 + kk) * N + pos] =
+          sm[((p * nlg + kk) << logn) + brv(src, logn)];
+    }
+  }
+}
+
+__global__ void pack_bytes_kernel(const uint8_t* __restrict__ bytes, uint16_t* __restrict__ coeffs, size_t groups) {
+  // pack_bytes_into_coeffs (dns/bucket.rs:289-303): 5 bytes -> 4 ten-bit coefficients
+  const size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= groups) return;
+  const uint8_t* s = bytes + gi * 5;
+  const uint64_t v = (uint64_t)s[0] | ((uint64_t)s[1] << 8) | ((uint64_t)s[2] << 16) | ((uint64_t)s[3] << 24) |
+                     ((uint64_t)s[4] << 32);
+  uint16_t* o = coeffs + gi * 4;
+  o[0] = (uint16_t)(v & 1023);
+  o[1] = (uint16_t)((v >> 10) & 1023);
+  o[2] = (uint16_t)((v >> 20) & 1023);
+  o[3] = (uint16_t)((v >> 30) & 1023);
+}
+
+// Device tables of 5^r and 5^-r mod 2N (r < N/2), one per log2n.
+struct PowTables {
+  uint32_t* pow5[LOG2_N_MAX + 1] = {};
+  uint32_t* pow5inv[LOG2_N_MAX + 1] = {};
+};
+
+}  // namespace
+
+// Host copies of the powers of 5 (computed once per process and device).
+static const uint32_t* pow_table(int log2n, bool inverse) {
+  static PowTables tabs[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  PowTables& pt = tabs[dev & 63];
+  uint32_t*& slot = inverse ? pt.pow5inv[log2n] : pt.pow5[log2n];
+  if (!slot) {
+    const uint32_t two_n = 2u << log2n;
+    std::vector<uint32_t> h(two_n / 4 + 1);
+    uint32_t inv5 = 1;
+    for (uint32_t x = 1; x < two_n; x += 2)
+      if ((5 * x) % two_n == 1) inv5 = x;
+    uint32_t base = inverse ? inv5 : 5, cur = 1;
+    for (size_t r = 0; r < h.size(); r++) {
+      h[r] = cur;
+      cur = (cur * base) % two_n;
+    }
+    uint32_t* d = nullptr;
+    if (cudaMalloc(&d, h.size() * 4) != cudaSuccess) return nullptr;
+    cudaMemcpy(d, h.data(), h.size() * 4, cudaMemcpyHostToDevice);
+    slot = d;
+  }
+  return slot;
+}
+
+void launch_encode_cols(const uint16_t* in, uint32_t* A, const Group& g, uint32_t l_in, int nl, const NttTables& T,
+                        cudaStream_t st) {
+  const uint32_t total = l_in * nl;
+  if (!total) return;
+  const int ppc = g.n >= 1024 ? 4 : 8;
+  const size_t smem = (size_t)ppc * g.n * 4;
+  const uint32_t blocks = (total + ppc - 1) / ppc;
+  set_smem(encode_cols_kernel, smem);
+  encode_cols_kernel<<<blocks, 256, smem, st>>>(in, A, g.log2n, total, ppc, T);
+}
+
+void launch_encode_rows(const uint32_t* A, uint32_t* Ahat, const Group& g, uint32_t l_in, int nl, const NttTables& T,
+                        cudaStream_t st) {
+  const int logn2 = g.log2n - __builtin_ctz(g.qbp);
+  const uint32_t n2 = 1u << logn2;
+  int U = 8;
+  while (U > 1 && (uint32_t)U > g.n) U >>= 1;
+  const size_t smem = (size_t)U * n2 * 4;
+  dim3 grid(g.n / U, nl);
+  set_smem(encode_rows_kernel, smem);
+  encode_rows_kernel<<<grid, 256, smem, st>>>(A, Ahat, g, l_in, nl, U, logn2, pow_table(g.log2n, false), T);
+}
+
+void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int nl, int frame, const NttTables& T,
+                        cudaStream_t st) {
+  uint32_t linv = 1;
+  for (uint32_t x = 1; x < TPLAIN; x++)
+    if ((x * (g.l % TPLAIN)) % TPLAIN == 1) linv = x;
+  const int nlg = nl < 8 ? nl : 8;
+  const size_t smem = (size_t)2 * nlg * g.n * 4;
+  dim3 grid(g.L, g.H, (nl + 7) / 8);
+  set_smem(encode_lift_kernel, smem);
+  encode_lift_kernel<<<grid, 512, smem, st>>>(Ahat, out, g, nl, frame, linv, pow_table(g.log2n, true), T);
+}
+
+void launch_pack_bytes(const uint8_t* bytes, uint16_t* coeffs, size_t entries, int log2n, cudaStream_t st) {
+  const size_t groups = entries * ((size_t)1 << log2n) / 4;
+  pack_bytes_kernel<<<(unsigned)((groups + 255) / 256), 256, 0, st>>>(bytes, coeffs, groups);
+}
+
+const uint32_t* device_pow5(int log2n, bool inverse) { return pow_table(log2n, inverse); }
+
+}  // namespace dnspir

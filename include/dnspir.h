@@ -1,0 +1,131 @@
+/* dnspir.h -- C ABI of the B200 answer path of DNSPIR's two-level BFV PIR.
+ *
+ * Drop-in boundary for the server side of FeanorTheElf/dnspir's crates/pir:
+ * the functions below replace the reference calls cited beside each one
+ * (paths relative to crates/pir/src/).  Plain pointers and sizes only; every
+ * function returns a status code (DNSPIR_OK = 0) and never aborts; the
+ * message of the last failure on the calling thread is dnspir_last_error().
+ * Host buffers belong to the caller, device memory to the library.  There is
+ * no CPU fallback: without a CUDA device every constructor fails with
+ * DNSPIR_ERR_CUDA.
+ *
+ * Ring elements cross the boundary as N coefficients in [0, q), q = q1 q2,
+ * q1 = 2^26 - 2^12 + 1, q2 = 2^25 - 2^12 + 1 (base_pir.rs:75-77), uint64 each.
+ * Plaintext entries are N coefficients in [0, 1025) (uint16), entry e of a
+ * database of group order l being element e of its 8 l entries (set_db order,
+ * base_pir.rs:612-637).
+ */
+#ifndef DNSPIR_H
+#define DNSPIR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DNSPIR_OK = 0,
+  DNSPIR_ERR_BAD_SIZE = 1,  /* byte or entry count wrong: uncondense "not enough data" (pir_wrapper.rs:124), set_db length (base_pir.rs:693) */
+  DNSPIR_ERR_BAD_SHAPE = 2, /* invalid group order / entry count / conjugate presence (base_pir.rs:150-154, pir_wrapper.rs:221-222, double_pir.rs:160) */
+  DNSPIR_ERR_OOM = 3,       /* device memory exhausted */
+  DNSPIR_ERR_CUDA = 4,      /* CUDA runtime error or no device */
+  DNSPIR_ERR_TIMEOUT = 5,   /* a bounded wait gave up */
+  DNSPIR_ERR_BAD_ARG = 6,   /* null pointer, index out of range, value not reduced */
+  DNSPIR_ERR_NOT_READY = 7  /* shard used before it was preprocessed */
+};
+
+const char* dnspir_last_error(void);
+const char* dnspir_version(void);
+
+/* ---- shape rules ------------------------------------------------------- */
+
+/* get_database_shape + num_databases (pir_wrapper.rs:219-241): group orders of
+ * the primary and secondary databases and the number of primary shards for a
+ * database of num_entries plaintext entries (N = 2048). */
+int dnspir_get_database_shape(uint64_t num_entries, uint32_t* primary_order, uint32_t* secondary_order,
+                              uint32_t* num_shards);
+/* choose_index_group_secondary (pir_wrapper.rs:166-175) */
+int dnspir_choose_secondary_order(uint32_t num_shards, uint32_t* secondary_order);
+/* PIRDatabase::required_memory_general (base_pir.rs:369-371), in 32-byte elements */
+uint64_t dnspir_required_memory_general(uint32_t log2_n, uint32_t group_order);
+/* byte length of a query (prepare_query_general output, pir_wrapper.rs:304-316) and of a reply (:401-408) */
+uint64_t dnspir_query_bytes(uint32_t primary_order, uint32_t secondary_order);
+uint64_t dnspir_reply_bytes(void);
+
+/* expand (bfv.rs:46-49) of SEEDS[which] (base_pir.rs:64-71) for ring dimension
+ * 2^log2_n: out = N coefficients in [0, q).  Host only; needs no device. */
+int dnspir_expand_seed(uint32_t log2_n, int which, uint64_t* out);
+
+/* ---- one preprocessed shard: PIRDatabase (base_pir.rs:229-255) --------- */
+
+typedef struct dnspir_db dnspir_db;
+
+/* PIRDatabase::create (base_pir.rs:280): used_seeds 0 = FirstSet, 1 = SecondSet
+ * (:104-107); the slab is allocated on `device`. */
+int dnspir_db_create(int device, uint32_t log2_n, uint32_t group_order, int used_seeds, dnspir_db** out);
+/* PIRDatabase::set_db (base_pir.rs:632): count must equal 8 * group_order * N
+ * coefficients; entries_on_device != 0 if `entries` is a device pointer. */
+int dnspir_db_set_db(dnspir_db* db, const uint16_t* entries, uint64_t count, int entries_on_device);
+/* PIRDatabase::get_a (base_pir.rs:897): out = 8 x N coefficients */
+int dnspir_db_get_a(dnspir_db* db, uint64_t* out);
+/* PIRDatabase::perform_pir_split (base_pir.rs:958): lane k answers query k.
+ * qry_b: 8 x N, qry_conj_b: 8 x N (NULL iff group_order < N), gk_b: 8 x 2 x N,
+ * out_b: 8 x N. */
+int dnspir_db_perform_pir_split(dnspir_db* db, const uint64_t* qry_b, const uint64_t* qry_conj_b,
+                                const uint64_t* gk_b, uint64_t* out_b);
+int dnspir_db_destroy(dnspir_db* db);
+
+/* ---- a fleet of primary shards and the two-level answer ---------------- */
+
+typedef struct dnspir_fleet dnspir_fleet;
+
+/* A fleet laid out by get_database_shape(num_entries) (N = 2048).  Only
+ * num_distinct shard slabs are stored; logical shard k is served by distinct
+ * shard k % num_distinct, as bench_wrapped_pir's preprocessed-db-count does
+ * (pir_wrapper.rs:578). */
+int dnspir_fleet_create(int device, uint64_t num_entries, uint32_t num_distinct, dnspir_fleet** out);
+/* The same with explicit shape (any N = 2^log2_n, 3 <= log2_n <= 11), as the
+ * reference's perform_double_pir tests use (double_pir.rs:328-451). */
+int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_order, uint32_t secondary_order,
+                                uint32_t num_shards, uint32_t num_distinct, dnspir_fleet** out);
+/* set_db of `count` distinct shards starting at first_distinct (base_pir.rs:632;
+ * dns/server.rs:707-728).  entries: count x (8 primary_order N) coefficients. */
+int dnspir_fleet_set_shards(dnspir_fleet* fleet, uint32_t first_distinct, uint32_t count, const uint16_t* entries,
+                            int entries_on_device);
+/* Synthetic 2560-byte payloads packed into 10-bit coefficients
+ * (pack_bytes_into_coeffs, dns/bucket.rs:289-303): bytes = entries x 2560 on
+ * the device, coeffs = entries x 2048 on the device. */
+int dnspir_pack_payloads(int device, const uint8_t* bytes, uint64_t entries, uint16_t* coeffs);
+
+/* process_queries (pir_wrapper.rs:349-409) for nq independent queries.
+ * queries[i] has query_lens[i] bytes; reply i is written at replies + i *
+ * reply_stride (dnspir_reply_bytes() bytes).  status[i] receives each query's
+ * status.  on_device != 0: query and reply buffers are device pointers. */
+int dnspir_fleet_process_queries(dnspir_fleet* fleet, const uint8_t* const* queries, const uint64_t* query_lens,
+                                 uint32_t nq, uint8_t* replies, uint64_t reply_stride, int32_t* status,
+                                 int on_device);
+/* process_query (pir_wrapper.rs:328) */
+int dnspir_fleet_process_query(dnspir_fleet* fleet, const uint8_t* query, uint64_t query_len, uint8_t* reply,
+                               uint64_t* reply_len);
+/* perform_double_pir (double_pir.rs:104-123) on ring elements: pq, pqc (NULL
+ * iff the primary group needs no conjugate), sq, sqc (likewise), gk (2 x N);
+ * out = 3 ciphertexts x (a, b) x N. */
+int dnspir_fleet_perform_double_pir(dnspir_fleet* fleet, const uint64_t* pq, const uint64_t* pqc, const uint64_t* sq,
+                                    const uint64_t* sqc, const uint64_t* gk, uint64_t* out);
+/* Device time of the last answered query, from CUDA events: primary phase
+ * (decode + scan + epilogue), secondary phase, and the scan kernel alone
+ * (PRIMARY_PHASE_MICROS / SECONDARY_PHASE_MICROS, double_pir.rs:230-242). */
+int dnspir_fleet_last_timings(dnspir_fleet* fleet, double* primary_ms, double* secondary_ms, double* scan_ms);
+/* Launch on a caller-owned cudaStream_t (NULL restores the fleet's own stream). */
+int dnspir_fleet_set_stream(dnspir_fleet* fleet, void* cuda_stream);
+/* Bytes of slab memory the fleet holds on its device. */
+uint64_t dnspir_fleet_slab_bytes(dnspir_fleet* fleet);
+int dnspir_fleet_destroy(dnspir_fleet* fleet);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DNSPIR_H */

@@ -1,0 +1,173 @@
+"""GPU parity: the CUDA path, through the C ABI, against the CPU oracle.
+
+Bit-exact equality of every output (integer arithmetic; no tolerance), plus the
+client's decryption of every answer, on the cases of the reference's own tests
+(N = 8 and 256, full group and subgroups; base_pir.rs:1281-1537,
+double_pir.rs:328-451) and on the CPU-runnable bench configuration (2^15
+entries of N = 2048, pir_wrapper.rs:493-615).
+"""
+import numpy as np
+import pytest
+
+import dnspir_b200 as dp
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+T = orc.T
+
+
+def _data(seed, rows, n):
+    return np.random.default_rng(seed).integers(0, T, size=(rows, n), dtype=np.uint16)
+
+
+def _monomial(n, e):
+    m = np.zeros(n, dtype=np.int64)
+    e %= 2 * n
+    if e < n:
+        m[e] = 1
+    else:
+        m[e - n] = T - 1
+    return m
+
+
+@pytest.mark.parametrize("log2n,l", [(3, 8), (3, 4), (3, 2), (8, 256), (8, 128), (8, 32), (8, 8)])
+def test_set_db_get_a_matches_oracle(log2n, l):
+    # preprocessing (set_transformed_entries + the partial_gal chain) end to end:
+    # get_a depends on every encoded entry and on every chain step
+    n = 1 << log2n
+    data = _data(l, 8 * l, n)
+    ref = orc.Database(log2n, l)
+    ref.set_db(data)
+    db = dp.PIRDatabase(log2n, l)
+    db.set_db(data)
+    assert np.array_equal(db.get_a().astype(np.int64), ref.get_a())
+
+
+@pytest.mark.parametrize("l", [256, 32])
+def test_perform_pir_split_matches_oracle(l):
+    # arbitrary ring elements as queries: checks the scan on every lane
+    log2n, n = 8, 256
+    data = _data(7 + l, 8 * l, n)
+    ref = orc.Database(log2n, l)
+    ref.set_db(data)
+    db = dp.PIRDatabase(log2n, l)
+    db.set_db(data)
+    gen = np.random.default_rng(l)
+    qb = gen.integers(0, orc.Q, size=(8, n), dtype=np.int64)
+    qc = gen.integers(0, orc.Q, size=(8, n), dtype=np.int64) if l == n else None
+    gk = gen.integers(0, orc.Q, size=(8, 2, n), dtype=np.int64)
+    want = ref.perform_pir_split(qb, qc, gk)
+    got = db.perform_pir_split(qb, qc, gk)
+    assert np.array_equal(got.astype(np.int64), want)
+
+
+def test_base_pir_split_decrypts():
+    # base_pir.rs:1496-1537 on the GPU: 8 clients, one per lane
+    n = 256
+    data = _data(3, 8 * n, n)
+    db = dp.PIRDatabase(8, n)
+    db.set_db(data)
+    rng = orc.Rng(bytes(32))
+    sks = [orc.gen_sk(rng, 8) for _ in range(8)]
+    gks = np.stack([orc.gen_gk_b(rng, 8, sks[i]) for i in range(8)])
+    a = db.get_a().astype(np.int64)
+    for idx in (0, 13, 255):
+        qbs = np.stack([orc.enc_sym_b(rng, 8, 2, sks[i], _monomial(n, idx)) for i in range(8)])
+        qcbs = np.stack([orc.enc_sym_b(rng, 8, 3, sks[i], _monomial(n, 2 * n - idx)) for i in range(8)])
+        b = db.perform_pir_split(qbs, qcbs, gks).astype(np.int64)
+        for i in range(8):
+            assert np.array_equal(orc.dec(8, sks[i], a[i], b[i]), data[idx * 8 + i].astype(np.int64))
+
+
+def _fleets(log2n, l1, l2, count, distinct, seed):
+    n = 1 << log2n
+    data = np.stack([_data(seed + i, 8 * l1, n) for i in range(distinct)])
+    refs = []
+    for i in range(distinct):
+        d = orc.Database(log2n, l1)
+        d.set_db(data[i])
+        refs.append(d)
+    fleet = dp.Fleet.general(log2n, l1, l2, count, distinct)
+    fleet.set_shards(0, data)
+    return data, [refs[k % distinct] for k in range(count)], fleet
+
+
+@pytest.mark.parametrize("l1,l2,count,distinct", [(256, 256, 1, 1), (128, 16, 2, 2), (256, 32, 4, 2)])
+def test_double_pir_matches_oracle_and_decrypts(l1, l2, count, distinct):
+    # double_pir.rs:328-451 (full groups, half-size primary + subgroup secondary)
+    log2n, n = 8, 256
+    data, refs, fleet = _fleets(log2n, l1, l2, count, distinct, 40 + l1 + count)
+    rng = orc.Rng(bytes([l2 % 256]) * 32)
+    sk = orc.gen_sk(rng, log2n)
+    per = 8 * l1
+    cases = [(0, 0), (1, count - 1), (per - 1, 0), (9, count // 2), (per - 1, count - 1)]
+    if count * 8 < l2:
+        cases.append((2, count))  # a shard beyond the fleet answers zero (double_pir.rs:382-386)
+    for (i, j) in cases:
+        pq, pqc, sq, sqc, gk = orc.enc_double_pir(rng, log2n, l1, l2, sk, i, j)
+        want = orc.perform_double_pir(refs, l2, pq, pqc, sq, sqc, gk)
+        got = fleet.perform_double_pir(pq, pqc, sq, sqc, gk)
+        assert np.array_equal(got.astype(np.int64), want), (i, j)
+        res = orc.dec_double_pir(log2n, sk, got.astype(np.int64).reshape(6, n))
+        expect = data[j % distinct][i] if j < count else np.zeros(n)
+        assert np.array_equal(res, expect.astype(np.int64)), (i, j)
+
+
+@pytest.fixture(scope="module")
+def config1():
+    # bench --db-entries 32768 --preprocessed-db-count 2 (pir_wrapper.rs:493-615)
+    entries = 32768
+    l1, l2, shards = dp.get_database_shape(entries)
+    assert (l1, l2, shards) == (1024, 32, 4)
+    data, refs, fleet = _fleets(11, l1, l2, shards, 2, 100)
+    return data, refs, fleet, l1, l2, shards
+
+
+def test_process_query_config1_bytes_match_oracle(config1):
+    data, refs, fleet, l1, l2, shards = config1
+    rng = orc.Rng(bytes([1]) + bytes(31))
+    indices = [(0, 0), (1, 0), (0, 1), (2742, 3), (8191, 2), (4000, 1)]
+    for (i, j) in indices:
+        q, seed = orc.prepare_query(rng, i, j % shards, l1, l2)
+        assert len(q) == 43008
+        want = orc.process_query(refs, q)
+        got = fleet.process_query(q)
+        assert len(got) == 22272
+        assert got == want, (i, j)
+        res = orc.process_reply(got, seed)
+        assert np.array_equal(res, data[(j % shards) % 2][i].astype(np.int64)), (i, j)
+
+
+def test_process_queries_batch_equals_single(config1):
+    data, refs, fleet, l1, l2, shards = config1
+    rng = orc.Rng(bytes([2]) + bytes(31))
+    qs = [orc.prepare_query(rng, 17 * k, k % shards, l1, l2) for k in range(4)]
+    batch = fleet.process_queries([q for q, _ in qs])
+    for (q, seed), r in zip(qs, batch):
+        assert r == fleet.process_query(q)
+
+
+def test_bad_query_length_is_rejected(config1):
+    _, _, fleet, l1, l2, _ = config1
+    rng = orc.Rng(bytes(32))
+    q, _ = orc.prepare_query(rng, 0, 0, l1, l2)
+    for bad in (q[:-1], q + b"\x00", b""):
+        with pytest.raises(dp.DnspirError) as e:
+            fleet.process_query(bad)
+        assert e.value.code == 1
+
+
+def test_unprepared_fleet_is_rejected():
+    fleet = dp.Fleet(32768, 2)
+    with pytest.raises(dp.DnspirError) as e:
+        fleet.process_query(bytes(43008))
+    assert e.value.code == 7
+
+
+def test_conjugate_presence_is_checked():
+    # double_pir.rs:160
+    data, refs, fleet = _fleets(8, 256, 256, 1, 1, 5)
+    z = np.zeros(256, dtype=np.uint64)
+    with pytest.raises(dp.DnspirError) as e:
+        fleet.perform_double_pir(z, None, z, z, np.zeros((2, 256), dtype=np.uint64))
+    assert e.value.code == 2
