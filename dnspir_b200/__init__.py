@@ -20,7 +20,7 @@ import numpy as np
 
 __all__ = [
     "DnspirError", "lib", "get_database_shape", "num_databases", "required_memory_general",
-    "choose_secondary_order", "expand_seed", "query_bytes", "reply_bytes", "PIRDatabase", "Fleet", "pack_payloads",
+    "choose_secondary_order", "expand_seed", "query_bytes", "prepare_query", "process_reply", "reply_bytes", "PIRDatabase", "Fleet", "pack_payloads",
     "LOG2_N", "N", "Q1", "Q2", "Q", "SIMD_COUNT", "PLAIN_MODULUS",
 ]
 
@@ -86,6 +86,9 @@ def lib():
         L.dnspir_fleet_slab_bytes.restype = c.c_uint64
         L.dnspir_fleet_slab_bytes.argtypes = [_vp]
         L.dnspir_fleet_destroy.argtypes = [_vp]
+        L.dnspir_client_prepare_query.argtypes = [c.c_char_p, c.c_uint64, c.c_uint64, c.c_uint32, c.c_uint32, _vp,
+                                                  _u64p, _vp]
+        L.dnspir_client_process_reply.argtypes = [_vp, c.c_uint64, c.c_char_p, _vp]
         _lib = L
     return _lib
 
@@ -148,6 +151,28 @@ def expand_seed(log2_n, which):
 def pack_payloads(payload, out, device=0):
     """pack_bytes_into_coeffs (dns/bucket.rs:289) on the device: uint8 (E, 2560) -> uint16 (E, 2048)."""
     _check(lib().dnspir_pack_payloads(device, _dev_ptr(payload), payload.shape[0], _dev_ptr(out)))
+
+
+def prepare_query(rng_seed, primary_idx, secondary_idx, primary_order, secondary_order):
+    """Client side, pir_wrapper.rs:276: (query bytes, 32-byte secret-key seed)."""
+    out = np.zeros(1 << 17, dtype=np.uint8)
+    n = ctypes.c_uint64()
+    sk = np.zeros(32, dtype=np.uint8)
+    rc = lib().dnspir_client_prepare_query(bytes(rng_seed), primary_idx, secondary_idx, primary_order,
+                                           secondary_order, _ptr(out), ctypes.byref(n), _ptr(sk))
+    if rc:
+        raise DnspirError(rc, "prepare_query: bad shape or index")
+    return out[: n.value].tobytes(), sk.tobytes()
+
+
+def process_reply(reply, sk_seed):
+    """Client side, pir_wrapper.rs:420: the N coefficients of the entry (uint16)."""
+    r = np.frombuffer(bytes(reply), dtype=np.uint8)
+    out = np.zeros(N, dtype=np.uint16)
+    rc = lib().dnspir_client_process_reply(_ptr(r), len(r), bytes(sk_seed), _ptr(out))
+    if rc:
+        raise DnspirError(rc, "process_reply: malformed reply")
+    return out
 
 
 def _zq(a, shape):

@@ -124,6 +124,17 @@ int dnspir_fleet_set_stream(dnspir_fleet* fleet, void* cuda_stream);
 uint64_t dnspir_fleet_slab_bytes(dnspir_fleet* fleet);
 int dnspir_fleet_destroy(dnspir_fleet* fleet);
 
+/* ---- client side (host only; load generation and answer checks) -------- */
+
+/* prepare_query_general (pir_wrapper.rs:276-317) with rng = StdRng(rng_seed):
+ * writes dnspir_query_bytes(primary_order, secondary_order) bytes and the
+ * 32-byte secret-key seed needed to read the reply. */
+int dnspir_client_prepare_query(const uint8_t* rng_seed, uint64_t primary_idx, uint64_t secondary_idx,
+                                uint32_t primary_order, uint32_t secondary_order, uint8_t* query,
+                                uint64_t* query_len, uint8_t* sk_seed_out);
+/* process_reply (pir_wrapper.rs:420-440): the N = 2048 coefficients of the entry. */
+int dnspir_client_process_reply(const uint8_t* reply, uint64_t reply_len, const uint8_t* sk_seed, uint16_t* coeffs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,8 @@ def _declare(L):
         L.orc_scan_baseline.restype = c.c_double
         L.orc_scan_baseline.argtypes = [c.c_int, c.c_uint32, c.c_uint32, c.c_int, c.c_int, _p(c.c_int)]
         L.orc_cpu_has_avx512.restype = c.c_int
+        L.orc_time_secondary.restype = c.c_double
+        L.orc_time_secondary.argtypes = [c.c_int, c.c_uint32]
 
 
 class OracleError(RuntimeError):
@@ -365,6 +367,11 @@ def scan_baseline(log2n, l, shards, threads, reps):
     used = ctypes.c_int()
     t = lib().orc_scan_baseline(log2n, l, shards, threads, reps, ctypes.byref(used))
     return t, used.value
+
+
+def time_secondary(log2n, l2):
+    """Seconds of one oracle secondary phase (set_db + scan) at secondary order l2."""
+    return lib().orc_time_secondary(log2n, l2)
 
 
 def cpu_has_avx512():

@@ -77,3 +77,30 @@ def test_no_cpu_fallback():
     with pytest.raises(dp.DnspirError) as e:
         dp.PIRDatabase(8, 256)
     assert e.value.code == 4
+
+
+@pytest.mark.parametrize("entries,i,j", [(32768, 0, 0), (32768, 8191, 3), (1 << 20, 12345, 63), (1 << 22, 16383, 255)])
+def test_client_query_matches_oracle_client(entries, i, j):
+    # the library's client (prepare_query, pir_wrapper.rs:276) produces the
+    # oracle client's bytes for the same StdRng seed
+    l1, l2, _ = dp.get_database_shape(entries)
+    seed = bytes([7, i % 256, j % 256]) + bytes(29)
+    q, sk = dp.prepare_query(seed, i, j, l1, l2)
+    q2, sk2 = orc.prepare_query(orc.Rng(seed), i, j, l1, l2)
+    assert q == q2 and sk == sk2
+    assert len(q) == dp.query_bytes(l1, l2)
+
+
+def test_client_reads_oracle_reply():
+    # process_reply (pir_wrapper.rs:420) of an oracle-made answer on a 1-shard 2^13 fleet
+    gen = np.random.default_rng(9)
+    data = gen.integers(0, orc.T, size=(8192, 2048), dtype=np.uint16)
+    db = orc.Database(11, 1024)
+    db.set_db(data)
+    l1, l2, s = dp.get_database_shape(8192)
+    for i in (0, 5000):
+        q, sk = dp.prepare_query(bytes([i % 256]) * 32, i, 0, l1, l2)
+        reply = orc.process_query([db], q)
+        assert np.array_equal(dp.process_reply(reply, sk), data[i])
+    with pytest.raises(dp.DnspirError):
+        dp.process_reply(reply[:-10], sk)
