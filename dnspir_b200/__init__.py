@@ -72,6 +72,7 @@ def lib():
         L.dnspir_db_get_a.argtypes = [_vp, _vp]
         L.dnspir_db_perform_pir_split.argtypes = [_vp, _vp, _vp, _vp, _vp]
         L.dnspir_db_destroy.argtypes = [_vp]
+        L.dnspir_db_perform_pir_split_noalloc.argtypes = [_vp] * 6
         L.dnspir_fleet_create.argtypes = [c.c_int, c.c_uint64, c.c_uint32, c.POINTER(_vp)]
         L.dnspir_fleet_create_general.argtypes = [c.c_int, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32,
                                                   c.c_uint32, c.POINTER(_vp)]

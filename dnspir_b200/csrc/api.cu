@@ -376,6 +376,19 @@ struct dnspir_fleet {
   }
 };
 
+// Read-only view of a shard for the no-allocation entry point (noalloc.cu).
+namespace dnspir {
+int db_view(const dnspir_db* db, DbView* out) {
+  out->device = db->device;
+  out->ready = db->ready;
+  out->g = db->g;
+  out->slab = db->slab;
+  out->T = db->ctx->T;
+  return DNSPIR_OK;
+}
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace dnspir
+
 // ============================================================== C ABI
 extern "C" {
 

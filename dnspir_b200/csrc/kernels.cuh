@@ -106,6 +106,15 @@ void launch_reply(const uint32_t* chain_out, int nq, int H, uint8_t* reply_bytes
 // Device table of 5^r (inverse: 5^-r) mod 2N for r <= N/2.
 const uint32_t* device_pow5(int log2n, bool inverse);
 
+// Read-only view of a shard (api.cu) for the no-allocation entry point (noalloc.cu).
+struct DbView {
+  int device;
+  bool ready;
+  Group g;
+  const uint32_t* slab;
+  NttTables T;
+};
+
 // Payload helpers for synthetic databases (dns/bucket.rs:289-303 packing).
 void launch_pack_bytes(const uint8_t* bytes, uint16_t* coeffs, size_t entries, int log2n, cudaStream_t st);
 

@@ -76,6 +76,19 @@ int dnspir_db_get_a(dnspir_db* db, uint64_t* out);
 int dnspir_db_perform_pir_split(dnspir_db* db, const uint64_t* qry_b, const uint64_t* qry_conj_b,
                                 const uint64_t* gk_b, uint64_t* out_b);
 int dnspir_db_destroy(dnspir_db* db);
+/* No counterpart in the reference.  The same answer as
+ * dnspir_db_perform_pir_split for callers that cannot allocate device memory
+ * while answering (HBM fully committed to shard slabs; request paths that must
+ * not call cudaMalloc, which can fail and synchronizes the device).  All five
+ * arrays are DEVICE pointers with the layouts of dnspir_db_perform_pir_split;
+ * coefficients must already be below q (not checked).  Work is queued on
+ * cuda_stream (NULL = the default stream) and the call returns without waiting.
+ * Intermediates live in a static 5 MiB region of device memory that every GPU
+ * loading the library holds until exit; nothing is allocated.  The first call
+ * on a device looks that region up (make it before any stream capture).  Calls
+ * on one device share the region: calls whose work overlaps on the GPU race. */
+int dnspir_db_perform_pir_split_noalloc(dnspir_db* db, const uint64_t* qry_b, const uint64_t* qry_conj_b,
+                                        const uint64_t* gk_b, uint64_t* out_b, void* cuda_stream);
 
 /* ---- a fleet of primary shards and the two-level answer ---------------- */
 
