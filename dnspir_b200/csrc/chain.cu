@@ -2,120 +2,335 @@
 // (crates/pir/src/base_pir.rs:496-594, 782-863) and its fusion with the
 // secondary scan (double_pir.rs:195-218).
 //
-// One block owns one (database, half, lane) chain; the ciphertext state stays
-// in shared memory for all loop_len steps.  A step is
-//     t      = sigma_5(a)                     (the galois lookup of :509-515)
-//     d0, d1 = balanced base-2^26 digits of the centred CRT lift of iNTT(t)
-//              (:541-571, copied exactly)
+// A chain step on the a-part of a ciphertext is
+//     t      = sigma_5(a)                        (the galois lookup of :509-515)
+//     v      = centred CRT lift of iNTT(t)        (:544-555)
+//     d1     = (v + 2^25) >> 26, d0 = v - 2^26 d1 (:557-570; the second digit's
+//              own carry is always 0 since |v| < q/2 < 2^50)
 //     a      = NTT(d0) gk_a0 + NTT(d1) gk_a1 + qry_a E_i
-// and, for the secondary database evaluated on a query ciphertext,
+// and, for the secondary database evaluated on a query ciphertext (b-part),
 //     b      = sigma_5(b) + NTT(d0) gk_b0 + NTT(d1) gk_b1 + qry_b E_i,
 // which is the homomorphic evaluation whose b-part main_pir_loop computes
 // from the stored digits (its sum/sum_new recurrence equals b up to the
 // sigma_5 applied before the final permute, :1072-1073).
 //
-// Shared-memory vectors hold NTT slots in bit-reversed position order
-// (position q <-> slot brv(q)); constants are stored the same way.
+// Because d0 + 2^26 d1 = v exactly and v = t in each factor, NTT(d0) =
+// t - 2^26 NTT(d1): one forward transform per factor and step instead of two.
+//
+// Layout: one 2-block cluster per chain, block rank p owning RNS factor p.
+// The blocks exchange their iNTT outputs through distributed shared memory
+// (double-buffered by step parity, one cluster barrier per step), each
+// computes the CRT lift and the high digit, and transforms it in its own
+// factor.  NTT-domain vectors hold slots in bit-reversed position order
+// (position q <-> slot brv(q)); the constants are stored the same way.
+#include <cooperative_groups.h>
+
+#include <cstring>
+
 #include "kernels.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace dnspir {
 namespace {
 
-constexpr int CHAIN_THREADS = 512;
-constexpr int PERM_REGS = (4 * N_MAX) / CHAIN_THREADS;
+constexpr int CT = 512;  // threads per block of a chain cluster
 
-// t = sigma_5(x) for `npoly` length-N vectors starting at sm (in place).
-__device__ __forceinline__ void galois_inplace(uint32_t* sm, int npoly, int logn, const uint32_t* __restrict__ galb) {
-  const int N = 1 << logn;
-  const int total = npoly << logn;
-  uint32_t regs[PERM_REGS];
-#pragma unroll
-  for (int c = 0; c < PERM_REGS; c++) {
-    const int e = threadIdx.x + c * CHAIN_THREADS;
-    if (e < total) regs[c] = sm[e];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < PERM_REGS; c++) {
-    const int e = threadIdx.x + c * CHAIN_THREADS;
-    if (e < total) sm[(e & ~(N - 1)) + __ldg(galb + (e & (N - 1)))] = regs[c];
-  }
-  __syncthreads();
+// ---- Montgomery arithmetic, R = 2^32 (p < 2^26)
+__host__ __device__ constexpr uint32_t neg_inv32(uint32_t p) {
+  uint32_t x = p;  // Newton iteration for p^-1 mod 2^32
+  for (int i = 0; i < 5; i++) x *= 2u - p * x;
+  return 0u - x;
+}
+// x * y R^-1 mod p for products and sums below 2^64 whose result is < 3p; returns [0, p)
+__device__ __forceinline__ uint32_t mont_reduce(uint64_t T, uint32_t p, uint32_t pinv) {
+  const uint32_t m = (uint32_t)T * pinv;
+  uint64_t u = (T + (uint64_t)m * p) >> 32;
+  u = u >= p ? u - p : u;
+  u = u >= p ? u - p : u;
+  return (uint32_t)u;
 }
 
-// digits of the centred CRT lift: src q1/q2 coefficient vectors -> dst[4][N]
-// ordered (d0 q1, d1 q1, d0 q2, d1 q2)
-__device__ __forceinline__ void decompose(const uint32_t* src1, const uint32_t* src2, uint32_t* dst, int logn,
-                                          CrtConst cc) {
-  const int N = 1 << logn;
-  for (int n = threadIdx.x; n < N; n += CHAIN_THREADS) {
-    const uint64_t v = crt(src1[n], src2[n], cc);
-    int64_t x = (int64_t)v;
-    if (v > QQ / 2) x -= (int64_t)QQ;
-    int64_t cur = x;
-    int64_t d[2];
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-      const int64_t high = (cur + ((int64_t)1 << (LOG2_B - 1))) >> LOG2_B;
-      d[k] = cur - high * ((int64_t)1 << LOG2_B);
-      cur = high;
-    }
-    dst[n] = smod(d[0], P1);
-    dst[N + n] = smod(d[1], P1);
-    dst[2 * N + n] = smod(d[0], P2);
-    dst[3 * N + n] = smod(d[1], P2);
-  }
-  __syncthreads();
-}
+struct ChainPrime {
+  uint32_t p, pinv;      // factor and -p^-1 mod 2^32
+  uint32_t r2;           // R^2 mod p (to enter Montgomery form)
+  uint32_t c26;          // 2^26 R mod p
+  uint32_t k1, k1q;      // q2^-1 N^-1 mod q1 with its Shoup companion (CRT, factor 1)
+  uint32_t k2, k2q;      // q1^-1 N^-1 mod q2 (CRT, factor 2)
+};
 
-__global__ void __launch_bounds__(CHAIN_THREADS) primary_chain_kernel(uint32_t* const* __restrict__ slabs,
-                                                                     uint32_t* __restrict__ a_out, Group g,
-                                                                     ChainConsts cc, NttTables T, CrtConst crtc,
-                                                                     uint32_t c_first, uint32_t cinv_first,
-                                                                     uint32_t inv5) {
-  extern __shared__ uint32_t sm[];  // [0,2N): a / t ; [2N,6N): digits
-  const int lane = blockIdx.x, h = blockIdx.y, s = blockIdx.z;
-  uint32_t* slab = slabs[s];
-  const int logn = g.log2n;
-  const uint32_t N = g.n, mask = 2 * N - 1;
-  uint32_t* dg = sm + 2 * N;
-  for (uint32_t b = threadIdx.x; b < 2 * N; b += CHAIN_THREADS) sm[b] = 0;
-  __syncthreads();
-  uint32_t ci = c_first;       // 5^(L-1-i) mod 2N
-  uint32_t cinv = cinv_first;  // 5^-(L-1-i) mod 2N
-  const uint32_t* gka0 = cc.gka;
-  const uint32_t* gka1 = cc.gka + 2 * N;
-  const uint32_t* qa = cc.qa + (size_t)h * 2 * N;
-  for (uint32_t i = 0; i < g.L; i++) {
-    galois_inplace(sm, 2, logn, cc.galb);
-    ntt_inv_smem2(sm, logn, 1, 1, T);
-    decompose(sm, sm + N, dg, logn, crtc);
-    ntt_fwd_smem2(dg, logn, 2, 2, T);
-    // key digits of row i in the scan layout: G'[i][k] = G_i[idx(5^(L-1-i) (2k+1))]
-    for (uint32_t b = threadIdx.x; b < 4 * N; b += CHAIN_THREADS) {
-      const uint32_t which = b >> logn, k = b & (N - 1);
-      const uint32_t p = which >> 1, d = which & 1;
-      const uint32_t j = gidx(ci * (2 * k + 1), mask);
-      slab[slab_off(g, p, h, i, 1 + d, k) + lane] = dg[(which << logn) + brv(j, logn)];
-    }
-    // a = d0 gk_a0 + d1 gk_a1 + qry_a E_i  (E_i read back from the scan layout)
-    for (uint32_t b = threadIdx.x; b < 2 * N; b += CHAIN_THREADS) {
-      const uint32_t p = b >> logn, pos = b & (N - 1);
-      const uint32_t j = brv(pos, logn);
-      const uint32_t ks = gidx(cinv * (2 * j + 1), mask);
-      const uint32_t e = slab[slab_off(g, p, h, i, 0, ks) + lane];
-      const uint32_t d0 = dg[((2 * p) << logn) + pos], d1 = dg[((2 * p + 1) << logn) + pos];
-      const uint32_t pr = prime_of(p);
-      const uint64_t acc = (uint64_t)d0 * __ldg(gka0 + b) + (uint64_t)d1 * __ldg(gka1 + b) +
-                           (uint64_t)e * __ldg(qa + b);
-      sm[b] = reduce64(acc, pr, barrett_mu(pr));
+// radix-4 / radix-2 transforms of one length-2^logn vector by CT threads.
+// Forward: natural -> bit-reversed (CT butterflies); inverse: bit-reversed ->
+// natural, NOT scaled by N^-1 (the caller folds N^-1 into its next constant).
+__device__ __forceinline__ void fwd_one(uint32_t* x, int logn, const uint32_t* __restrict__ tw,
+                                        const uint32_t* __restrict__ twq, uint32_t p) {
+  const int N = 1 << logn;
+  int s = 0;
+  for (; s + 1 < logn; s += 2) {
+    const int t = N >> (s + 1), t2 = t >> 1, m = 1 << s;
+    for (int g = threadIdx.x; g < N / 4; g += CT) {
+      const int blk = g / t2, r = g - blk * t2;
+      const int j = blk * 2 * t + r;
+      uint32_t x0 = x[j], x1 = x[j + t2], x2 = x[j + t], x3 = x[j + t + t2];
+      const uint32_t w = tw[m + blk], wq = twq[m + blk];
+      uint32_t v = shoup_mul(x2, w, wq, p);
+      x2 = sub_mod(x0, v, p);
+      x0 = add_mod(x0, v, p);
+      v = shoup_mul(x3, w, wq, p);
+      x3 = sub_mod(x1, v, p);
+      x1 = add_mod(x1, v, p);
+      const uint32_t wa = tw[2 * m + 2 * blk], waq = twq[2 * m + 2 * blk];
+      const uint32_t wb = tw[2 * m + 2 * blk + 1], wbq = twq[2 * m + 2 * blk + 1];
+      v = shoup_mul(x1, wa, waq, p);
+      x[j + t2] = sub_mod(x0, v, p);
+      x[j] = add_mod(x0, v, p);
+      v = shoup_mul(x3, wb, wbq, p);
+      x[j + t + t2] = sub_mod(x2, v, p);
+      x[j + t] = add_mod(x2, v, p);
     }
     __syncthreads();
-    ci = (ci * inv5) & mask;
-    cinv = (cinv * 5) & mask;
   }
-  uint32_t* o = a_out + (((size_t)s * g.H + h) * SIMD + lane) * 2 * N;
-  for (uint32_t b = threadIdx.x; b < 2 * N; b += CHAIN_THREADS) o[b] = sm[b];
+  if (s < logn) {  // last stage, t = 1
+    for (int b = threadIdx.x; b < N / 2; b += CT) {
+      const int j = 2 * b;
+      const uint32_t v = shoup_mul(x[j + 1], tw[N / 2 + b], twq[N / 2 + b], p);
+      const uint32_t u = x[j];
+      x[j] = add_mod(u, v, p);
+      x[j + 1] = sub_mod(u, v, p);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void inv_one(uint32_t* x, int logn, const uint32_t* __restrict__ tw,
+                                        const uint32_t* __restrict__ twq, uint32_t p) {
+  const int N = 1 << logn;
+  int s = 0;
+  for (; s + 1 < logn; s += 2) {
+    const int t = 1 << s;
+    const int h0 = N >> (s + 1), h1 = N >> (s + 2);
+    for (int g = threadIdx.x; g < N / 4; g += CT) {
+      const int blk = g >> s, r = g & (t - 1);
+      const int j = (blk << (s + 2)) + r;
+      uint32_t x0 = x[j], x1 = x[j + t], x2 = x[j + 2 * t], x3 = x[j + 3 * t];
+      const uint32_t wa = tw[h0 + 2 * blk], waq = twq[h0 + 2 * blk];
+      const uint32_t wb = tw[h0 + 2 * blk + 1], wbq = twq[h0 + 2 * blk + 1];
+      uint32_t u = add_mod(x0, x1, p);
+      x1 = shoup_mul(sub_mod(x0, x1, p), wa, waq, p);
+      x0 = u;
+      u = add_mod(x2, x3, p);
+      x3 = shoup_mul(sub_mod(x2, x3, p), wb, wbq, p);
+      x2 = u;
+      const uint32_t w = tw[h1 + blk], wq = twq[h1 + blk];
+      x[j] = add_mod(x0, x2, p);
+      x[j + 2 * t] = shoup_mul(sub_mod(x0, x2, p), w, wq, p);
+      x[j + t] = add_mod(x1, x3, p);
+      x[j + 3 * t] = shoup_mul(sub_mod(x1, x3, p), w, wq, p);
+    }
+    __syncthreads();
+  }
+  if (s < logn) {  // last stage, t = N/2
+    const uint32_t w = tw[1], wq = twq[1];
+    for (int j = threadIdx.x; j < N / 2; j += CT) {
+      const uint32_t u = x[j], v = x[j + N / 2];
+      x[j] = add_mod(u, v, p);
+      x[j + N / 2] = shoup_mul(sub_mod(u, v, p), w, wq, p);
+    }
+    __syncthreads();
+  }
+}
+
+// high digit of the centred CRT lift from the two factors' unscaled iNTT outputs
+__device__ __forceinline__ int32_t high_digit(uint32_t c1, uint32_t c2, const ChainPrime& P1c, const ChainPrime& P2c) {
+  const uint32_t x1 = shoup_mul(c1, P1c.k1, P1c.k1q, P1);
+  const uint32_t x2 = shoup_mul(c2, P2c.k2, P2c.k2q, P2);
+  uint64_t v = (uint64_t)x1 * P2 + (uint64_t)x2 * P1;
+  v = v >= QQ ? v - QQ : v;
+  int64_t x = (int64_t)v;
+  if (v > QQ / 2) x -= (int64_t)QQ;
+  return (int32_t)((x + ((int64_t)1 << (LOG2_B - 1))) >> LOG2_B);
+}
+
+struct ChainArgs {
+  Group g;
+  // constants: gk_a digits [d][p][pos], qry_a halves [h][p][pos], sigma_5 map, canonical
+  const uint32_t* gka;
+  const uint32_t* qa;
+  const uint32_t* galb;
+  NttTables T;
+  ChainPrime cp[2];
+  // secondary: entries in chain layout, query vectors [q][slot][p][pos], output
+  const uint32_t* E;
+  const uint32_t* qv;
+  size_t qv_stride;
+  int nl;
+  uint32_t* out;
+  // primary: slabs and a-part output
+  uint32_t* const* slabs;
+  uint32_t* a_out;
+  uint32_t c_first, cinv_first, inv5;
+};
+
+// Shared-memory plan (u32 words, N = 2^logn):
+//   A, TC, D           N each    state a, saved sigma_5(a), work vector
+//   X[2]               2N        iNTT outputs published to the peer block
+//   CG0, CG1, CQA      3N        gk_a0 R, gk_a1 R, qry_a R of this factor and half
+//   FW, FWQ, IW, IWQ   4N        twiddles of this factor
+//   B, QG0, QG1, QQB   4N        b, gk_b0 R, gk_b1 R, qry_b R (secondary only)
+template <bool SECONDARY>
+__device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, int q, int s, uint32_t* sm) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int p = (int)cluster.block_rank();
+  const int logn = a.g.log2n;
+  const int N = 1 << logn;
+  const uint32_t mask = 2 * N - 1;
+  const ChainPrime cp = a.cp[p];
+  const uint32_t pr = cp.p;
+  uint32_t* A = sm;
+  uint32_t* TC = A + N;
+  uint32_t* D = TC + N;
+  uint32_t* X = D + N;
+  uint32_t* CG0 = X + 2 * N;
+  uint32_t* CG1 = CG0 + N;
+  uint32_t* CQA = CG1 + N;
+  uint32_t* FW = CQA + N;
+  uint32_t* FWQ = FW + N;
+  uint32_t* IW = FWQ + N;
+  uint32_t* IWQ = IW + N;
+  uint32_t* B = IWQ + N;
+  uint32_t* QG0 = B + N;
+  uint32_t* QG1 = QG0 + N;
+  uint32_t* QQB = QG1 + N;
+  for (int b = threadIdx.x; b < N; b += CT) {
+    A[b] = 0;
+    if (SECONDARY) B[b] = 0;
+    const size_t o = (size_t)p * N + b;
+    CG0[b] = mont_reduce((uint64_t)a.gka[o] * cp.r2, pr, cp.pinv);
+    CG1[b] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
+    CQA[b] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, pr, cp.pinv);
+    if (SECONDARY) {
+      const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
+      QG0[b] = mont_reduce((uint64_t)qq[o] * cp.r2, pr, cp.pinv);
+      QG1[b] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
+      QQB[b] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, pr, cp.pinv);
+    }
+    FW[b] = a.T.fw[p][b];
+    FWQ[b] = a.T.fwq[p][b];
+    IW[b] = a.T.iw[p][b];
+    IWQ[b] = a.T.iwq[p][b];
+  }
+  cluster.sync();
+  uint32_t* peerX = cluster.map_shared_rank(X, p ^ 1);
+  uint32_t* slab = SECONDARY ? nullptr : a.slabs[s];
+  uint32_t ci = a.c_first, cinv = a.cinv_first;
+  constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
+  for (uint32_t i = 0; i < a.g.L; i++) {
+    // entries of row i for this thread's positions, consumed at the end of the step
+    uint32_t e[PER];
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      e[c] = 0;
+      if (pos < N) {
+        if (SECONDARY) {
+          e[c] = __ldg(a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + lane) * N + pos);
+        } else {
+          const uint32_t j = brv(pos, logn);
+          const uint32_t ks = gidx(cinv * (2 * j + 1), mask);
+          e[c] = slab[slab_off(a.g, p, h, i, 0, ks) + lane];
+        }
+      }
+    }
+    // sigma_5 on a (and b)
+    uint32_t ra[PER], rb[PER];
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      if (pos < N) {
+        ra[c] = A[pos];
+        if (SECONDARY) rb[c] = B[pos];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      if (pos < N) {
+        const uint32_t dst = __ldg(a.galb + pos);
+        TC[dst] = ra[c];
+        D[dst] = ra[c];
+        if (SECONDARY) B[dst] = rb[c];
+      }
+    }
+    __syncthreads();
+    inv_one(D, logn, IW, IWQ, pr);
+    uint32_t* Xc = X + (i & 1) * N;
+    for (int b = threadIdx.x; b < N; b += CT) Xc[b] = D[b];
+    cluster.sync();
+    const uint32_t* Pc = peerX + (i & 1) * N;
+    for (int b = threadIdx.x; b < N; b += CT) {
+      const uint32_t own = D[b], other = Pc[b];
+      const int32_t hd = p == 0 ? high_digit(own, other, a.cp[0], a.cp[1]) : high_digit(other, own, a.cp[0], a.cp[1]);
+      D[b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
+    }
+    __syncthreads();
+    fwd_one(D, logn, FW, FWQ, pr);
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      if (pos < N) {
+        const uint32_t n1 = D[pos];
+        const uint32_t n0 = sub_mod(TC[pos], mont_reduce((uint64_t)n1 * cp.c26, pr, cp.pinv), pr);
+        A[pos] = mont_reduce((uint64_t)n0 * CG0[pos] + (uint64_t)n1 * CG1[pos] + (uint64_t)e[c] * CQA[pos], pr,
+                             cp.pinv);
+        if (SECONDARY) {
+          B[pos] = mont_reduce(((uint64_t)B[pos] << 32) + (uint64_t)n0 * QG0[pos] + (uint64_t)n1 * QG1[pos] +
+                                   (uint64_t)e[c] * QQB[pos],
+                               pr, cp.pinv);
+        } else {
+          TC[pos] = n0;
+        }
+      }
+    }
+    __syncthreads();
+    if (!SECONDARY) {
+      // key digits of row i in the scan layout: G'[i][k] = G_i[idx(5^(L-1-i) (2k+1))]
+      for (int k = threadIdx.x; k < N; k += CT) {
+        const uint32_t jb = brv(gidx(ci * (2 * k + 1), mask), logn);
+        slab[slab_off(a.g, p, h, i, 1, k) + lane] = TC[jb];
+        slab[slab_off(a.g, p, h, i, 2, k) + lane] = D[jb];
+      }
+      // TC and D are rewritten only after the next step's first barrier
+      ci = (ci * a.inv5) & mask;
+      cinv = (cinv * 5) & mask;
+    }
+  }
+  if (SECONDARY) {
+    uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + lane % CTXT_PARTS) * 2) * 2 * N;
+    for (int b = threadIdx.x; b < N; b += CT) {
+      o[(size_t)p * N + b] = A[b];
+      o[2 * (size_t)N + (size_t)p * N + b] = B[b];
+    }
+  } else {
+    uint32_t* o = a.a_out + (((size_t)s * a.g.H + h) * SIMD + lane) * 2 * N;
+    for (int b = threadIdx.x; b < N; b += CT) o[(size_t)p * N + b] = A[b];
+  }
+  cluster.sync();  // keep this block's shared memory alive until the peer's last read
+}
+
+// grid: x = factor (cluster of 2), y = part * H + half, z = query
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT)
+    secondary_chain_kernel(ChainArgs a) {
+  extern __shared__ uint32_t sm[];
+  const int h = blockIdx.y % a.g.H, part = blockIdx.y / a.g.H, q = blockIdx.z;
+  chain_body<true>(a, h, q * CTXT_PARTS + part, q, 0, sm);
+}
+
+// grid: x = factor (cluster of 2), y = lane * H + half, z = shard
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT) primary_chain_kernel(ChainArgs a) {
+  extern __shared__ uint32_t sm[];
+  const int h = blockIdx.y % a.g.H, lane = blockIdx.y / a.g.H;
+  chain_body<false>(a, h, lane, 0, blockIdx.z, sm);
 }
 
 // reply_a = a_main + a_conj -> iNTT -> CRT; also the 17-bit mod switch
@@ -140,60 +355,20 @@ __global__ void primary_finalize_kernel(const uint32_t* __restrict__ a_out, uint
   }
 }
 
-// Secondary database evaluated on each query ciphertext.  Block: (query,
-// half, part).  State a, b and digits in shared memory: [0,2N) a, [2N,4N) b,
-// [4N,8N) digits.
-__global__ void __launch_bounds__(CHAIN_THREADS) secondary_chain_kernel(const uint32_t* __restrict__ E,
-                                                                       const uint32_t* __restrict__ qv,
-                                                                       size_t qv_stride, int nl,
-                                                                       uint32_t* __restrict__ out, Group g,
-                                                                       ChainConsts cc, NttTables T, CrtConst crtc) {
-  extern __shared__ uint32_t sm[];
-  const int part = blockIdx.x, h = blockIdx.y, q = blockIdx.z;
-  const int lane = q * CTXT_PARTS + part;
-  const int logn = g.log2n;
-  const uint32_t N = g.n;
-  uint32_t* a = sm;
-  uint32_t* bb = sm + 2 * N;
-  uint32_t* dg = sm + 4 * N;
-  for (uint32_t b = threadIdx.x; b < 4 * N; b += CHAIN_THREADS) sm[b] = 0;
-  __syncthreads();
-  const uint32_t* gka0 = cc.gka;
-  const uint32_t* gka1 = cc.gka + 2 * N;
-  const uint32_t* qa = cc.qa + (size_t)h * 2 * N;
-  // decoded query vectors, slots [gk0, gk1, pq, pqc, sq, sqc] each [p][pos]
-  const uint32_t* qq = qv + (size_t)q * qv_stride;
-  const uint32_t* gkb0 = qq;
-  const uint32_t* gkb1 = qq + 2 * N;
-  const uint32_t* qb = qq + (size_t)(4 + h) * 2 * N;
-  for (uint32_t i = 0; i < g.L; i++) {
-    galois_inplace(sm, 4, logn, cc.galb);
-    ntt_inv_smem2(a, logn, 1, 1, T);
-    decompose(a, a + N, dg, logn, crtc);
-    ntt_fwd_smem2(dg, logn, 2, 2, T);
-    const uint32_t* Ei = E + ((((size_t)0 * g.H + h) * g.L + i) * nl + lane) * N;
-    const size_t pstride = (size_t)g.H * g.L * nl * N;
-    for (uint32_t b = threadIdx.x; b < 2 * N; b += CHAIN_THREADS) {
-      const uint32_t p = b >> logn, pos = b & (N - 1);
-      const uint32_t e = __ldg(Ei + p * pstride + pos);
-      const uint32_t d0 = dg[((2 * p) << logn) + pos], d1 = dg[((2 * p + 1) << logn) + pos];
-      const uint32_t pr = prime_of(p);
-      const uint64_t mu = barrett_mu(pr);
-      const uint64_t acc_a = (uint64_t)d0 * __ldg(gka0 + b) + (uint64_t)d1 * __ldg(gka1 + b) +
-                             (uint64_t)e * __ldg(qa + b);
-      const uint64_t acc_b = (uint64_t)bb[b] + (uint64_t)d0 * __ldg(gkb0 + b) + (uint64_t)d1 * __ldg(gkb1 + b) +
-                             (uint64_t)e * __ldg(qb + b);
-      a[b] = reduce64(acc_a, pr, mu);
-      bb[b] = reduce64(acc_b, pr, mu);
-    }
-    __syncthreads();
-  }
-  uint32_t* o = out + ((((size_t)q * g.H + h) * CTXT_PARTS + part) * 2) * 2 * N;
-  for (uint32_t b = threadIdx.x; b < 4 * N; b += CHAIN_THREADS) o[b] = sm[b];
-}
-
 }  // namespace
 
+CrtConst host_crt_const();
+
+static uint64_t pw(uint64_t b, uint64_t e, uint64_t m) {
+  uint64_t r = 1 % m;
+  b %= m;
+  while (e) {
+    if (e & 1) r = (uint64_t)((unsigned __int128)r * b % m);
+    b = (uint64_t)((unsigned __int128)b * b % m);
+    e >>= 1;
+  }
+  return r;
+}
 static uint32_t pow_mod2n(uint32_t b, uint32_t e, uint32_t mask) {
   uint32_t r = 1;
   for (uint32_t k = 0; k < e; k++) r = (r * b) & mask;
@@ -205,19 +380,46 @@ static uint32_t inv5_mod2n(uint32_t two_n) {
   return 1;
 }
 
-CrtConst host_crt_const();
+static ChainArgs chain_args(const Group& g, const ChainConsts& cc, const NttTables& T) {
+  ChainArgs a;
+  memset(&a, 0, sizeof(a));
+  a.g = g;
+  a.gka = cc.gka;
+  a.qa = cc.qa;
+  a.galb = cc.galb;
+  a.T = T;
+  const uint64_t n = g.n;
+  const CrtConst crtc = host_crt_const();
+  for (int p = 0; p < 2; p++) {
+    ChainPrime& c = a.cp[p];
+    c.p = p ? P2 : P1;
+    c.pinv = neg_inv32(c.p);
+    c.r2 = (uint32_t)pw(pw(2, 64, c.p), 1, c.p);
+    c.c26 = (uint32_t)((((unsigned __int128)1 << 26) << 32) % c.p);
+    const uint64_t ninv1 = pw(n, P1 - 2, P1), ninv2 = pw(n, P2 - 2, P2);
+    c.k1 = (uint32_t)((uint64_t)crtc.q2inv1 * ninv1 % P1);
+    c.k1q = (uint32_t)(((uint64_t)c.k1 << 32) / P1);
+    c.k2 = (uint32_t)((uint64_t)crtc.q1inv2 * ninv2 % P2);
+    c.k2q = (uint32_t)(((uint64_t)c.k2 << 32) / P2);
+  }
+  return a;
+}
+
+static size_t chain_smem(const Group& g, bool secondary) { return (size_t)(secondary ? 16 : 12) * g.n * 4; }
 
 void launch_primary_chain(uint32_t* const* slabs_dev, int nshards, uint32_t* a_out, const Group& g,
                           const ChainConsts& cc, const NttTables& T, cudaStream_t st) {
+  ChainArgs a = chain_args(g, cc, T);
+  a.slabs = slabs_dev;
+  a.a_out = a_out;
   const uint32_t mask = 2 * g.n - 1;
-  const uint32_t inv5 = inv5_mod2n(2 * g.n);
-  const uint32_t c_first = pow_mod2n(5, g.L - 1, mask);
-  const uint32_t cinv_first = pow_mod2n(inv5, g.L - 1, mask);
-  const size_t smem = (size_t)6 * g.n * 4;
+  a.inv5 = inv5_mod2n(2 * g.n);
+  a.c_first = pow_mod2n(5, g.L - 1, mask);
+  a.cinv_first = pow_mod2n(a.inv5, g.L - 1, mask);
+  const size_t smem = chain_smem(g, false);
   set_smem(primary_chain_kernel, smem);
-  dim3 grid(SIMD, g.H, nshards);
-  primary_chain_kernel<<<grid, CHAIN_THREADS, smem, st>>>(slabs_dev, a_out, g, cc, T, host_crt_const(), c_first,
-                                                          cinv_first, inv5);
+  dim3 grid(2, SIMD * g.H, nshards);
+  primary_chain_kernel<<<grid, CT, smem, st>>>(a);
 }
 
 void launch_primary_finalize(const uint32_t* a_out, int nshards, uint64_t* a_zq, uint32_t* a_ms, const Group& g,
@@ -229,11 +431,16 @@ void launch_primary_finalize(const uint32_t* a_out, int nshards, uint64_t* a_zq,
 
 void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_stride, int nq, uint32_t* out,
                             const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st) {
-  const size_t smem = (size_t)8 * g.n * 4;
+  ChainArgs a = chain_args(g, cc, T);
+  a.E = E;
+  a.qv = qv;
+  a.qv_stride = qv_stride;
+  a.nl = nq * CTXT_PARTS;
+  a.out = out;
+  const size_t smem = chain_smem(g, true);
   set_smem(secondary_chain_kernel, smem);
-  dim3 grid(CTXT_PARTS, g.H, nq);
-  secondary_chain_kernel<<<grid, CHAIN_THREADS, smem, st>>>(E, qv, qv_stride, nq * CTXT_PARTS, out, g, cc, T,
-                                                            host_crt_const());
+  dim3 grid(2, CTXT_PARTS * g.H, nq);
+  secondary_chain_kernel<<<grid, CT, smem, st>>>(a);
 }
 
 }  // namespace dnspir
