@@ -84,6 +84,7 @@ def lib():
         L.dnspir_fleet_perform_double_pir.argtypes = [_vp] * 7
         L.dnspir_fleet_last_timings.argtypes = [_vp] + [c.POINTER(c.c_double)] * 3
         L.dnspir_fleet_set_stream.argtypes = [_vp, _vp]
+        L.dnspir_fleet_batch_timings.argtypes = [_vp, c.c_uint32] + [_vp] * 4
         L.dnspir_fleet_slab_bytes.restype = c.c_uint64
         L.dnspir_fleet_slab_bytes.argtypes = [_vp]
         L.dnspir_fleet_destroy.argtypes = [_vp]
@@ -333,6 +334,14 @@ class Fleet:
         a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _check(lib().dnspir_fleet_last_timings(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
+
+    def batch_timings(self, max_queries=1 << 16):
+        """Per-query (latency, primary, secondary, scan) ms of the last call, from CUDA events."""
+        out = np.full((4, max_queries), -1.0)
+        n = lib().dnspir_fleet_batch_timings(self._h, max_queries, *[_ptr(out[i]) for i in range(4)])
+        if n < 0:
+            _check(-n)
+        return out[:, :n]
 
     def set_stream(self, stream_handle):
         _check(lib().dnspir_fleet_set_stream(self._h, _vp(stream_handle) if stream_handle else None))

@@ -2,6 +2,7 @@
 // (twiddles, expanded a-parts), shards (PIRDatabase), fleets and the
 // two-level answer pipeline (perform_batched_double_pir, double_pir.rs:126-228;
 // process_queries, pir_wrapper.rs:349-409).
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -350,28 +351,63 @@ struct DeviceGuard {
   }
 };
 
+// RAII pinned host buffer (asynchronous copies need page-locked memory)
+struct HBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~HBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  int ensure(size_t b) {
+    if (b <= bytes) return DNSPIR_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    CK(cudaMallocHost(&p, b));
+    bytes = b;
+    return DNSPIR_OK;
+  }
+};
+
 // ------------------------------------------------------------------ fleet
+// Buffers of one query in flight.  Two slots alternate by query parity so that
+// the primary phase of query k+1 (main stream) overlaps the secondary phase of
+// query k (secondary stream); events order the reuse of a slot.
+struct QSlot {
+  DBuf qbytes, qnat, qbrv, sec_in, reply_dev;
+  HBuf qpin;  // host staging of the query bytes
+  cudaEvent_t prim_done = nullptr, sec_done = nullptr;
+  bool sec_pending = false, prim_recorded = false;
+};
+
 struct dnspir_fleet {
   int device = 0;
   DeviceCtx* ctx = nullptr;
   Group g1, g2;
   uint32_t S = 0, D = 0;
-  cudaStream_t own = nullptr, st = nullptr;
+  cudaStream_t own = nullptr, st = nullptr, sec = nullptr;
   std::vector<uint32_t*> slabs;
   std::vector<bool> ready;
   DBuf slabs_dev, distinct_dev, a_zq, a_ms;
   EncodeWs ws;
-  // per-query workspace
-  DBuf qbytes, qnat, qbrv, qzq, part, sec_in, secE, chain_out, reply_dev, reply_zq;
+  QSlot slot[2];
+  DBuf part, secE, chain_out, qzq, reply_zq;  // used by one stream at a time
+  HBuf rpin;                                  // host staging of the replies of one call
   int R = 1;
-  cudaEvent_t ev[5] = {};
-  bool have_times = false;
+  std::vector<cudaEvent_t> tev;  // 6 timing events per query of the last call
+  std::vector<int> tev_ok;
+  uint32_t tev_n = 0;
   std::mutex mu;
   ~dnspir_fleet() {
     for (uint32_t* s : slabs)
       if (s) cudaFree(s);
-    for (auto& e : ev)
+    for (auto& e : tev)
       if (e) cudaEventDestroy(e);
+    for (auto& s : slot) {
+      if (s.prim_done) cudaEventDestroy(s.prim_done);
+      if (s.sec_done) cudaEventDestroy(s.sec_done);
+    }
+    if (sec) cudaStreamDestroy(sec);
     if (own) cudaStreamDestroy(own);
   }
 };
@@ -571,8 +607,18 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   f->S = num_shards;
   f->D = num_distinct;
   CK(cudaStreamCreateWithFlags(&f->own, cudaStreamNonBlocking));
+  {
+    // the secondary phase runs at the highest priority so that its few,
+    // long-lived chain blocks are dispatched ahead of pending scan blocks
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&f->sec, cudaStreamNonBlocking, hi));
+  }
   f->st = f->own;
-  for (auto& e : f->ev) CK(cudaEventCreate(&e));
+  for (auto& s : f->slot) {
+    CK(cudaEventCreateWithFlags(&s.prim_done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s.sec_done, cudaEventDisableTiming));
+  }
   f->slabs.assign(num_distinct, nullptr);
   f->ready.assign(num_distinct, false);
   const size_t words = slab_words(f->g1);
@@ -625,59 +671,102 @@ int dnspir_fleet_set_shards(dnspir_fleet* f, uint32_t first, uint32_t count, con
   return DNSPIR_OK;
 }
 
-// The answer pipeline for one query whose decoded vectors sit in f->qnat /
-// f->qbrv; writes either the reply bytes (reply_bytes) or Z_q ciphertexts.
-static int answer_one(dnspir_fleet* f, uint8_t* reply_bytes, uint64_t* reply_zq) {
-  const Group& g1 = f->g1;
-  const Group& g2 = f->g2;
-  const uint32_t n = g1.n;
-  cudaStream_t st = f->st;
-  const int chunks = g1.H * f->R;
-  CKR(f->part.ensure((size_t)chunks * f->S * 2 * n * SIMD * 4));
-  CKR(f->sec_in.ensure((size_t)g2.l * CTXT_PARTS * n * 2));
-  CKR(f->ws.A.ensure((size_t)g2.l * CTXT_PARTS * n * 4));
-  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * CTXT_PARTS * n * 4));
-  CKR(f->secE.ensure((size_t)2 * g2.H * g2.L * CTXT_PARTS * n * 4));
-  CKR(f->chain_out.ensure((size_t)g2.H * CTXT_PARTS * 2 * 2 * n * 4));
-  CK(cudaEventRecord(f->ev[1], st));
-  launch_scan_plain(f->slabs_dev.as<uint32_t*>(), f->S, f->qnat.as<uint32_t>(), f->part.as<uint32_t>(), g1, f->R, st);
-  CK(cudaEventRecord(f->ev[2], st));
-  launch_primary_epilogue(f->part.as<uint32_t>(), chunks, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
-                          f->sec_in.as<uint16_t>(), CTXT_PARTS, 0, g1, f->ctx->T, st);
-  CK(cudaEventRecord(f->ev[3], st));
-  const uint32_t l_in = f->S * SIMD;
-  launch_encode_cols(f->sec_in.as<uint16_t>(), f->ws.A.as<uint32_t>(), g2, l_in, CTXT_PARTS, f->ctx->T, st);
-  launch_encode_rows(f->ws.A.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, CTXT_PARTS, f->ctx->T, st);
-  launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, CTXT_PARTS, 1, f->ctx->T, st);
-  launch_secondary_chain(f->secE.as<uint32_t>(), f->qbrv.as<uint32_t>(), (size_t)6 * 2 * n, 1,
-                         f->chain_out.as<uint32_t>(), g2, chain_consts(f->ctx, g2.log2n, 1), f->ctx->T, st);
-  launch_reply(f->chain_out.as<uint32_t>(), 1, g2.H, reply_bytes, 0, reply_zq, g2.log2n, f->ctx->T, st);
-  CK(cudaEventRecord(f->ev[4], st));
-  CK(cudaGetLastError());
-  f->have_times = true;
-  return DNSPIR_OK;
-}
-
 static int fleet_ready(dnspir_fleet* f) {
   for (uint32_t d = 0; d < f->D; d++)
     if (!f->ready[d]) return fail(DNSPIR_ERR_NOT_READY, "fleet shard not preprocessed");
   return DNSPIR_OK;
 }
 
-static int fleet_workspace(dnspir_fleet* f) {
-  const uint32_t n = f->g1.n;
-  CKR(f->qnat.ensure((size_t)6 * 2 * n * 4));
-  CKR(f->qbrv.ensure((size_t)6 * 2 * n * 4));
+// Timing events of query i of the current call (created on demand).
+static int query_events(dnspir_fleet* f, uint32_t i, cudaEvent_t** out) {
+  while (f->tev.size() < 6 * (size_t)(i + 1)) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    f->tev.push_back(e);
+  }
+  if (f->tev_ok.size() < (size_t)i + 1) f->tev_ok.resize(i + 1, 0);
+  *out = &f->tev[6 * (size_t)i];
   return DNSPIR_OK;
 }
 
-static int process_one(dnspir_fleet* f, const uint8_t* q, uint64_t qlen, uint8_t* reply, int on_device) {
+static int slot_workspace(dnspir_fleet* f, QSlot& s) {
+  const uint32_t n = f->g1.n;
+  CKR(s.qnat.ensure((size_t)6 * 2 * n * 4));
+  CKR(s.qbrv.ensure((size_t)6 * 2 * n * 4));
+  CKR(s.sec_in.ensure((size_t)f->g2.l * CTXT_PARTS * n * 2));
+  return DNSPIR_OK;
+}
+
+// Primary phase of one query on the main stream: the slot's decoded vectors
+// (already written by `load`, which runs first) -> scan of every shard ->
+// epilogue into the slot's secondary entries.  Events: t[1] scan start,
+// t[2] scan end, t[3] primary end.
+static int stage_primary(dnspir_fleet* f, QSlot& s, cudaEvent_t* t) {
   const Group& g1 = f->g1;
-  const Group& g2 = f->g2;
-  if (g1.log2n != LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_SHAPE, "the wire format is defined for N = 2048");
-  const uint64_t want = dnspir_query_bytes(g1.l, g2.l);
-  if (qlen != want) return fail(DNSPIR_ERR_BAD_SIZE, "query length does not match the database shape");
   const uint32_t n = g1.n;
+  cudaStream_t st = f->st;
+  const int chunks = g1.H * f->R;
+  CKR(f->part.ensure((size_t)chunks * f->S * 2 * n * SIMD * 4));
+  if (t) CK(cudaEventRecord(t[1], st));
+  launch_scan_plain(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), f->part.as<uint32_t>(), g1, f->R, st);
+  if (t) CK(cudaEventRecord(t[2], st));
+  launch_primary_epilogue(f->part.as<uint32_t>(), chunks, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
+                          s.sec_in.as<uint16_t>(), CTXT_PARTS, 0, g1, f->ctx->T, st);
+  if (t) CK(cudaEventRecord(t[3], st));
+  CK(cudaEventRecord(s.prim_done, st));
+  s.prim_recorded = true;
+  CK(cudaGetLastError());
+  return DNSPIR_OK;
+}
+
+// Secondary phase on the secondary stream: encode the per-query database,
+// run the fused key-switch chain, write the reply (bytes, or Z_q ciphertexts),
+// and copy reply bytes to the host when host_reply is given.  Events: t[4]
+// secondary start, t[5] end.
+static int stage_secondary(dnspir_fleet* f, QSlot& s, cudaEvent_t* t, uint8_t* reply_dev, uint64_t* reply_zq,
+                           uint8_t* host_reply) {
+  const Group& g2 = f->g2;
+  const uint32_t n = g2.n;
+  cudaStream_t st = f->sec;
+  CKR(f->ws.A.ensure((size_t)g2.l * CTXT_PARTS * n * 4));
+  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * CTXT_PARTS * n * 4));
+  CKR(f->secE.ensure((size_t)2 * g2.H * g2.L * CTXT_PARTS * n * 4));
+  CKR(f->chain_out.ensure((size_t)g2.H * CTXT_PARTS * 2 * 2 * n * 4));
+  CK(cudaStreamWaitEvent(st, s.prim_done, 0));
+  if (t) CK(cudaEventRecord(t[4], st));
+  const uint32_t l_in = f->S * SIMD;
+  launch_encode_cols(s.sec_in.as<uint16_t>(), f->ws.A.as<uint32_t>(), g2, l_in, CTXT_PARTS, f->ctx->T, st);
+  launch_encode_rows(f->ws.A.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, CTXT_PARTS, f->ctx->T, st);
+  launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, CTXT_PARTS, 1, f->ctx->T, st);
+  launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>(), (size_t)6 * 2 * n, 1,
+                         f->chain_out.as<uint32_t>(), g2, chain_consts(f->ctx, g2.log2n, 1), f->ctx->T, st);
+  launch_reply(f->chain_out.as<uint32_t>(), 1, g2.H, reply_dev, 0, reply_zq, g2.log2n, f->ctx->T, st);
+  if (host_reply) CK(cudaMemcpyAsync(host_reply, reply_dev, dnspir_reply_bytes(), cudaMemcpyDeviceToHost, st));
+  if (t) CK(cudaEventRecord(t[5], st));
+  CK(cudaEventRecord(s.sec_done, st));
+  s.sec_pending = true;
+  CK(cudaGetLastError());
+  return DNSPIR_OK;
+}
+
+// Before a slot is reused, the main stream waits for the slot's previous
+// secondary phase (it reads the slot's decoded vectors and entries).
+static int slot_acquire(dnspir_fleet* f, QSlot& s) {
+  if (s.sec_pending) CK(cudaStreamWaitEvent(f->st, s.sec_done, 0));
+  s.sec_pending = false;
+  return DNSPIR_OK;
+}
+
+// End of a call: the main stream waits for every secondary phase, then the host.
+static int fleet_drain(dnspir_fleet* f) {
+  for (auto& s : f->slot)
+    if (s.sec_pending) CK(cudaStreamWaitEvent(f->st, s.sec_done, 0));
+  CK(cudaStreamSynchronize(f->st));
+  for (auto& s : f->slot) s.sec_pending = false;
+  return DNSPIR_OK;
+}
+
+static PolySpec wire_spec(const Group& g1, const Group& g2) {
   PolySpec spec;
   memset(&spec, 0, sizeof(spec));
   uint32_t off = 0;
@@ -686,7 +775,7 @@ static int process_one(dnspir_fleet* f, const uint8_t* q, uint64_t qlen, uint8_t
     spec.bits[spec.npoly] = bits;
     spec.slot[spec.npoly] = slot;
     spec.npoly++;
-    off += n * bits / 8;
+    off += g1.n * bits / 8;
   };
   add(0, GK_BITS);
   add(1, GK_BITS);
@@ -694,23 +783,7 @@ static int process_one(dnspir_fleet* f, const uint8_t* q, uint64_t qlen, uint8_t
   if (g1.H == 2) add(3, PQ_BITS);
   add(4, SQ_BITS);
   if (g2.H == 2) add(5, SQ_BITS);
-  CKR(fleet_workspace(f));
-  const uint8_t* src = q;
-  CK(cudaEventRecord(f->ev[0], f->st));
-  if (!on_device) {
-    CKR(f->qbytes.ensure(want));
-    CK(cudaMemcpyAsync(f->qbytes.p, q, want, cudaMemcpyHostToDevice, f->st));
-    src = f->qbytes.as<uint8_t>();
-  }
-  launch_decode_query(src, spec, f->qnat.as<uint32_t>(), f->qbrv.as<uint32_t>(), g1.log2n, f->ctx->T, f->st);
-  uint8_t* dst = reply;
-  if (!on_device) {
-    CKR(f->reply_dev.ensure(dnspir_reply_bytes()));
-    dst = f->reply_dev.as<uint8_t>();
-  }
-  CKR(answer_one(f, dst, nullptr));
-  if (!on_device) CK(cudaMemcpyAsync(reply, dst, dnspir_reply_bytes(), cudaMemcpyDeviceToHost, f->st));
-  return DNSPIR_OK;
+  return spec;
 }
 
 int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries, const uint64_t* query_lens,
@@ -720,12 +793,56 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
   if (nq && reply_stride < dnspir_reply_bytes()) return fail(DNSPIR_ERR_BAD_ARG, "reply stride too small");
   std::lock_guard<std::mutex> lk(f->mu);
   CKR(fleet_ready(f));
+  const Group& g1 = f->g1;
+  const Group& g2 = f->g2;
+  if (g1.log2n != LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_SHAPE, "the wire format is defined for N = 2048");
   DeviceGuard dg(f->device);
+  const uint64_t want = dnspir_query_bytes(g1.l, g2.l);
+  const PolySpec spec = wire_spec(g1, g2);
+  f->tev_n = 0;
+  std::fill(f->tev_ok.begin(), f->tev_ok.end(), 0);
+  const size_t RB = dnspir_reply_bytes();
+  if (!on_device) CKR(f->rpin.ensure((size_t)nq * RB));
   int first_err = DNSPIR_OK;
   std::string first_msg;
+  uint32_t k = 0;  // answered queries so far (slot parity)
   for (uint32_t i = 0; i < nq; i++) {
-    int r = queries[i] ? process_one(f, queries[i], query_lens[i], replies + (size_t)i * reply_stride, on_device)
-                       : fail(DNSPIR_ERR_BAD_ARG, "null query");
+    int r = DNSPIR_OK;
+    if (!queries[i]) r = fail(DNSPIR_ERR_BAD_ARG, "null query");
+    else if (query_lens[i] != want) r = fail(DNSPIR_ERR_BAD_SIZE, "query length does not match the database shape");
+    cudaEvent_t* t = nullptr;
+    if (r == DNSPIR_OK) r = query_events(f, i, &t);
+    if (r == DNSPIR_OK) {
+      QSlot& s = f->slot[k & 1];
+      r = slot_acquire(f, s);
+      if (r == DNSPIR_OK) r = slot_workspace(f, s);
+      if (r == DNSPIR_OK && !on_device) {
+        r = s.qbytes.ensure(want);
+        if (r == DNSPIR_OK) r = s.qpin.ensure(want);
+        if (r == DNSPIR_OK) r = s.reply_dev.ensure(RB);
+        // the slot's staging buffer may still feed the copy of the query two back
+        if (r == DNSPIR_OK && s.prim_recorded && cudaEventSynchronize(s.prim_done) != cudaSuccess)
+          r = fail(DNSPIR_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+        if (r == DNSPIR_OK) memcpy(s.qpin.p, queries[i], want);
+      }
+      if (r == DNSPIR_OK) {
+        cudaError_t e = cudaEventRecord(t[0], f->st);
+        const uint8_t* src = queries[i];
+        if (e == cudaSuccess && !on_device) {
+          e = cudaMemcpyAsync(s.qbytes.p, s.qpin.p, want, cudaMemcpyHostToDevice, f->st);
+          src = s.qbytes.as<uint8_t>();
+        }
+        if (e != cudaSuccess) r = fail(DNSPIR_ERR_CUDA, cudaGetErrorString(e));
+        else launch_decode_query(src, spec, s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), g1.log2n, f->ctx->T, f->st);
+      }
+      if (r == DNSPIR_OK) r = stage_primary(f, s, t);
+      if (r == DNSPIR_OK)
+        r = on_device ? stage_secondary(f, s, t, replies + (size_t)i * reply_stride, nullptr, nullptr)
+                      : stage_secondary(f, s, t, s.reply_dev.as<uint8_t>(), nullptr, (uint8_t*)f->rpin.p + i * RB);
+      if (r == DNSPIR_OK) k++;
+      f->tev_ok[i] = r == DNSPIR_OK;
+      f->tev_n = i + 1;
+    }
     if (status) status[i] = r;
     if (r == DNSPIR_ERR_CUDA || r == DNSPIR_ERR_OOM) return r;
     if (r != DNSPIR_OK && first_err == DNSPIR_OK) {
@@ -733,7 +850,11 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
       first_msg = g_err;
     }
   }
-  CK(cudaStreamSynchronize(f->st));
+  CKR(fleet_drain(f));
+  if (!on_device)
+    for (uint32_t i = 0; i < nq; i++)
+      if (i < f->tev_ok.size() && f->tev_ok[i] && i < f->tev_n)
+        memcpy(replies + (size_t)i * reply_stride, (uint8_t*)f->rpin.p + i * RB, RB);
   if (first_err != DNSPIR_OK) g_err = first_msg;
   return first_err;
 }
@@ -767,32 +888,67 @@ int dnspir_fleet_perform_double_pir(dnspir_fleet* f, const uint64_t* pq, const u
   if (sqc) memcpy(&z[5 * n], sqc, n * 8);
   if (!reduced(z.data(), z.size())) return fail(DNSPIR_ERR_BAD_ARG, "ring element coefficients must be below q");
   DeviceGuard dg(f->device);
-  CKR(fleet_workspace(f));
+  QSlot& s = f->slot[0];
+  cudaEvent_t* t = nullptr;
+  CKR(query_events(f, 0, &t));
+  CKR(slot_acquire(f, s));
+  CKR(slot_workspace(f, s));
   CKR(f->qzq.ensure(z.size() * 8));
   CKR(f->reply_zq.ensure((size_t)CTXT_PARTS * 2 * n * 8));
-  CK(cudaEventRecord(f->ev[0], f->st));
+  CK(cudaEventRecord(t[0], f->st));
   CK(cudaMemcpyAsync(f->qzq.p, z.data(), z.size() * 8, cudaMemcpyHostToDevice, f->st));
-  launch_ring_to_ntt(f->qzq.as<uint64_t>(), 6, f->qnat.as<uint32_t>(), f->qbrv.as<uint32_t>(), f->g1.log2n,
-                     f->ctx->T, f->st);
-  CKR(answer_one(f, nullptr, f->reply_zq.as<uint64_t>()));
-  CK(cudaMemcpyAsync(out, f->reply_zq.p, (size_t)CTXT_PARTS * 2 * n * 8, cudaMemcpyDeviceToHost, f->st));
-  CK(cudaStreamSynchronize(f->st));
+  launch_ring_to_ntt(f->qzq.as<uint64_t>(), 6, s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), f->g1.log2n, f->ctx->T,
+                     f->st);
+  CKR(stage_primary(f, s, t));
+  CKR(stage_secondary(f, s, t, nullptr, f->reply_zq.as<uint64_t>(), nullptr));
+  f->tev_ok[0] = 1;
+  f->tev_n = 1;
+  CKR(fleet_drain(f));
+  CK(cudaMemcpy(out, f->reply_zq.p, (size_t)CTXT_PARTS * 2 * n * 8, cudaMemcpyDeviceToHost));
   return DNSPIR_OK;
+}
+
+int dnspir_fleet_batch_timings(dnspir_fleet* f, uint32_t max, double* latency_ms, double* primary_ms,
+                               double* secondary_ms, double* scan_ms) {
+  if (!f) return -fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  DeviceGuard dg(f->device);
+  const uint32_t n = f->tev_n < max ? f->tev_n : max;
+  for (uint32_t i = 0; i < n; i++) {
+    double v[4] = {-1, -1, -1, -1};
+    if (f->tev_ok[i]) {
+      cudaEvent_t* t = &f->tev[6 * (size_t)i];
+      float a = 0, b = 0, c = 0, d = 0;
+      if (cudaEventSynchronize(t[5]) != cudaSuccess || cudaEventElapsedTime(&a, t[0], t[5]) != cudaSuccess ||
+          cudaEventElapsedTime(&b, t[0], t[3]) != cudaSuccess || cudaEventElapsedTime(&c, t[4], t[5]) != cudaSuccess ||
+          cudaEventElapsedTime(&d, t[1], t[2]) != cudaSuccess) {
+        cudaGetLastError();
+        return -fail(DNSPIR_ERR_CUDA, "timing events unavailable");
+      }
+      v[0] = a, v[1] = b, v[2] = c, v[3] = d;
+    }
+    if (latency_ms) latency_ms[i] = v[0];
+    if (primary_ms) primary_ms[i] = v[1];
+    if (secondary_ms) secondary_ms[i] = v[2];
+    if (scan_ms) scan_ms[i] = v[3];
+  }
+  return (int)n;
 }
 
 int dnspir_fleet_last_timings(dnspir_fleet* f, double* primary_ms, double* secondary_ms, double* scan_ms) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
-  std::lock_guard<std::mutex> lk(f->mu);
-  if (!f->have_times) return fail(DNSPIR_ERR_NOT_READY, "no query answered yet");
-  DeviceGuard dg(f->device);
-  CK(cudaEventSynchronize(f->ev[4]));
-  float a = 0, b = 0, c = 0;
-  CK(cudaEventElapsedTime(&a, f->ev[0], f->ev[3]));
-  CK(cudaEventElapsedTime(&b, f->ev[3], f->ev[4]));
-  CK(cudaEventElapsedTime(&c, f->ev[1], f->ev[2]));
-  if (primary_ms) *primary_ms = a;
-  if (secondary_ms) *secondary_ms = b;
-  if (scan_ms) *scan_ms = c;
+  uint32_t n = 0;
+  {
+    std::lock_guard<std::mutex> lk(f->mu);
+    n = f->tev_n;
+    if (!n || !f->tev_ok[n - 1]) return fail(DNSPIR_ERR_NOT_READY, "no query answered yet");
+  }
+  std::vector<double> p(n), s(n), c(n);
+  const int got = dnspir_fleet_batch_timings(f, n, nullptr, p.data(), s.data(), c.data());
+  if (got < 0) return -got;
+  if (primary_ms) *primary_ms = p[n - 1];
+  if (secondary_ms) *secondary_ms = s[n - 1];
+  if (scan_ms) *scan_ms = c[n - 1];
   return DNSPIR_OK;
 }
 
@@ -809,6 +965,7 @@ int dnspir_fleet_destroy(dnspir_fleet* f) {
   if (!f) return DNSPIR_OK;
   DeviceGuard dg(f->device);
   cudaStreamSynchronize(f->st);
+  cudaStreamSynchronize(f->sec);
   delete f;
   return DNSPIR_OK;
 }

@@ -59,47 +59,65 @@ struct ChainPrime {
   uint32_t k2, k2q;      // q1^-1 N^-1 mod q2 (CRT, factor 2)
 };
 
-// radix-4 / radix-2 transforms of one length-2^logn vector by CT threads.
-// Forward: natural -> bit-reversed (CT butterflies); inverse: bit-reversed ->
-// natural, NOT scaled by N^-1 (the caller folds N^-1 into its next constant).
+// radix-4 / radix-2 transforms of one length-2^logn vector by CT threads, with
+// Harvey's lazy butterflies: values stay in [0, 4p) inside a transform (4p <
+// 2^28) and are brought back to [0, p) when it ends.
+// Forward: natural -> bit-reversed (CT butterflies), input in [0, p).
+// Inverse: bit-reversed -> natural, NOT scaled by N^-1 (the caller folds N^-1
+// into its next constant), input in [0, p).
+__device__ __forceinline__ uint32_t shoup_lazy(uint32_t x, uint32_t w, uint32_t wq, uint32_t p) {
+  return x * w - __umulhi(x, wq) * p;  // in [0, 2p) for any x < 2^32
+}
+__device__ __forceinline__ uint32_t red2p(uint32_t x, uint32_t p2) { return x >= p2 ? x - p2 : x; }
+// CT butterfly on [0, 4p) inputs: (x, y) -> (x + w y, x - w y), outputs in [0, 4p)
+__device__ __forceinline__ void ct_bf(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
+  const uint32_t a = red2p(x, 2 * p);
+  const uint32_t t = shoup_lazy(y, w, wq, p);
+  x = a + t;
+  y = a - t + 2 * p;
+}
+// GS butterfly on [0, 2p) inputs: (x, y) -> (x + y, w (x - y)), outputs in [0, 2p)
+__device__ __forceinline__ void gs_bf(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
+  const uint32_t a = x + y;
+  const uint32_t d = x - y + 2 * p;
+  x = red2p(a, 2 * p);
+  y = shoup_lazy(d, w, wq, p);
+}
+
 __device__ __forceinline__ void fwd_one(uint32_t* x, int logn, const uint32_t* __restrict__ tw,
                                         const uint32_t* __restrict__ twq, uint32_t p) {
   const int N = 1 << logn;
   int s = 0;
   for (; s + 1 < logn; s += 2) {
-    const int t = N >> (s + 1), t2 = t >> 1, m = 1 << s;
+    const int logt2 = logn - s - 2;
+    const int t2 = 1 << logt2, t = 2 * t2, m = 1 << s;
     for (int g = threadIdx.x; g < N / 4; g += CT) {
-      const int blk = g / t2, r = g - blk * t2;
-      const int j = blk * 2 * t + r;
+      const int blk = g >> logt2, r = g & (t2 - 1);
+      const int j = (blk << (logt2 + 2)) + r;
       uint32_t x0 = x[j], x1 = x[j + t2], x2 = x[j + t], x3 = x[j + t + t2];
       const uint32_t w = tw[m + blk], wq = twq[m + blk];
-      uint32_t v = shoup_mul(x2, w, wq, p);
-      x2 = sub_mod(x0, v, p);
-      x0 = add_mod(x0, v, p);
-      v = shoup_mul(x3, w, wq, p);
-      x3 = sub_mod(x1, v, p);
-      x1 = add_mod(x1, v, p);
-      const uint32_t wa = tw[2 * m + 2 * blk], waq = twq[2 * m + 2 * blk];
-      const uint32_t wb = tw[2 * m + 2 * blk + 1], wbq = twq[2 * m + 2 * blk + 1];
-      v = shoup_mul(x1, wa, waq, p);
-      x[j + t2] = sub_mod(x0, v, p);
-      x[j] = add_mod(x0, v, p);
-      v = shoup_mul(x3, wb, wbq, p);
-      x[j + t + t2] = sub_mod(x2, v, p);
-      x[j + t] = add_mod(x2, v, p);
+      ct_bf(x0, x2, w, wq, p);
+      ct_bf(x1, x3, w, wq, p);
+      ct_bf(x0, x1, tw[2 * m + 2 * blk], twq[2 * m + 2 * blk], p);
+      ct_bf(x2, x3, tw[2 * m + 2 * blk + 1], twq[2 * m + 2 * blk + 1], p);
+      x[j] = x0;
+      x[j + t2] = x1;
+      x[j + t] = x2;
+      x[j + t + t2] = x3;
     }
     __syncthreads();
   }
   if (s < logn) {  // last stage, t = 1
     for (int b = threadIdx.x; b < N / 2; b += CT) {
-      const int j = 2 * b;
-      const uint32_t v = shoup_mul(x[j + 1], tw[N / 2 + b], twq[N / 2 + b], p);
-      const uint32_t u = x[j];
-      x[j] = add_mod(u, v, p);
-      x[j + 1] = sub_mod(u, v, p);
+      uint32_t u = x[2 * b], v = x[2 * b + 1];
+      ct_bf(u, v, tw[N / 2 + b], twq[N / 2 + b], p);
+      x[2 * b] = u;
+      x[2 * b + 1] = v;
     }
     __syncthreads();
   }
+  for (int b = threadIdx.x; b < N; b += CT) x[b] = red2p(red2p(x[b], 2 * p), p);
+  __syncthreads();
 }
 
 __device__ __forceinline__ void inv_one(uint32_t* x, int logn, const uint32_t* __restrict__ tw,
@@ -113,31 +131,29 @@ __device__ __forceinline__ void inv_one(uint32_t* x, int logn, const uint32_t* _
       const int blk = g >> s, r = g & (t - 1);
       const int j = (blk << (s + 2)) + r;
       uint32_t x0 = x[j], x1 = x[j + t], x2 = x[j + 2 * t], x3 = x[j + 3 * t];
-      const uint32_t wa = tw[h0 + 2 * blk], waq = twq[h0 + 2 * blk];
-      const uint32_t wb = tw[h0 + 2 * blk + 1], wbq = twq[h0 + 2 * blk + 1];
-      uint32_t u = add_mod(x0, x1, p);
-      x1 = shoup_mul(sub_mod(x0, x1, p), wa, waq, p);
-      x0 = u;
-      u = add_mod(x2, x3, p);
-      x3 = shoup_mul(sub_mod(x2, x3, p), wb, wbq, p);
-      x2 = u;
+      gs_bf(x0, x1, tw[h0 + 2 * blk], twq[h0 + 2 * blk], p);
+      gs_bf(x2, x3, tw[h0 + 2 * blk + 1], twq[h0 + 2 * blk + 1], p);
       const uint32_t w = tw[h1 + blk], wq = twq[h1 + blk];
-      x[j] = add_mod(x0, x2, p);
-      x[j + 2 * t] = shoup_mul(sub_mod(x0, x2, p), w, wq, p);
-      x[j + t] = add_mod(x1, x3, p);
-      x[j + 3 * t] = shoup_mul(sub_mod(x1, x3, p), w, wq, p);
+      gs_bf(x0, x2, w, wq, p);
+      gs_bf(x1, x3, w, wq, p);
+      x[j] = x0;
+      x[j + t] = x1;
+      x[j + 2 * t] = x2;
+      x[j + 3 * t] = x3;
     }
     __syncthreads();
   }
   if (s < logn) {  // last stage, t = N/2
     const uint32_t w = tw[1], wq = twq[1];
     for (int j = threadIdx.x; j < N / 2; j += CT) {
-      const uint32_t u = x[j], v = x[j + N / 2];
-      x[j] = add_mod(u, v, p);
-      x[j + N / 2] = shoup_mul(sub_mod(u, v, p), w, wq, p);
+      uint32_t u = x[j], v = x[j + N / 2];
+      gs_bf(u, v, w, wq, p);
+      x[j] = u;
+      x[j + N / 2] = v;
     }
     __syncthreads();
   }
+  // outputs are in [0, 2p); the consumer (high_digit via Shoup) accepts any value < 2^32
 }
 
 // high digit of the centred CRT lift from the two factors' unscaled iNTT outputs

@@ -128,9 +128,17 @@ int dnspir_fleet_process_query(dnspir_fleet* fleet, const uint8_t* query, uint64
 int dnspir_fleet_perform_double_pir(dnspir_fleet* fleet, const uint64_t* pq, const uint64_t* pqc, const uint64_t* sq,
                                     const uint64_t* sqc, const uint64_t* gk, uint64_t* out);
 /* Device time of the last answered query, from CUDA events: primary phase
- * (decode + scan + epilogue), secondary phase, and the scan kernel alone
- * (PRIMARY_PHASE_MICROS / SECONDARY_PHASE_MICROS, double_pir.rs:230-242). */
+ * (copy-in + decode + scan + epilogue), secondary phase, and the scan kernel
+ * alone (PRIMARY_PHASE_MICROS / SECONDARY_PHASE_MICROS, double_pir.rs:230-242). */
 int dnspir_fleet_last_timings(dnspir_fleet* fleet, double* primary_ms, double* secondary_ms, double* scan_ms);
+/* Per-query device times of the last process_queries / perform_double_pir
+ * call, from CUDA events, for up to `max` queries: latency (start of the
+ * query's copy-in to its reply), primary phase, secondary phase, scan kernel.
+ * Consecutive queries overlap (the primary phase of query k+1 runs during the
+ * secondary phase of query k).  Entries of rejected queries are -1.  Returns
+ * the number of entries written, or minus a status code. */
+int dnspir_fleet_batch_timings(dnspir_fleet* fleet, uint32_t max, double* latency_ms, double* primary_ms,
+                               double* secondary_ms, double* scan_ms);
 /* Launch on a caller-owned cudaStream_t (NULL restores the fleet's own stream). */
 int dnspir_fleet_set_stream(dnspir_fleet* fleet, void* cuda_stream);
 /* Bytes of slab memory the fleet holds on its device. */
