@@ -84,6 +84,7 @@ def lib():
         L.dnspir_fleet_perform_double_pir.argtypes = [_vp] * 7
         L.dnspir_fleet_last_timings.argtypes = [_vp] + [c.POINTER(c.c_double)] * 3
         L.dnspir_fleet_set_stream.argtypes = [_vp, _vp]
+        L.dnspir_fleet_set_batch.argtypes = [_vp, c.c_uint32]
         L.dnspir_fleet_batch_timings.argtypes = [_vp, c.c_uint32] + [_vp] * 4
         L.dnspir_fleet_slab_bytes.restype = c.c_uint64
         L.dnspir_fleet_slab_bytes.argtypes = [_vp]
@@ -342,6 +343,10 @@ class Fleet:
         if n < 0:
             _check(-n)
         return out[:, :n]
+
+    def set_batch(self, max_batch):
+        """Queries per pass over the slabs (1, 2, 4, 8, 16); replies do not depend on it."""
+        _check(lib().dnspir_fleet_set_batch(self._h, max_batch))
 
     def set_stream(self, stream_handle):
         _check(lib().dnspir_fleet_set_stream(self._h, _vp(stream_handle) if stream_handle else None))

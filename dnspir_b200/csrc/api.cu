@@ -10,32 +10,18 @@
 #include <string>
 #include <vector>
 
-#include "dnspir.h"
-#include "kernels.cuh"
+#include "host.h"
 
 using namespace dnspir;
 
+namespace dnspir {
+
 // ------------------------------------------------------------------ errors
-static thread_local std::string g_err;
-static int fail(int code, const std::string& msg) {
+thread_local std::string g_err;
+int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
-#define CK(call)                                                                                           \
-  do {                                                                                                     \
-    cudaError_t e_ = (call);                                                                               \
-    if (e_ != cudaSuccess) {                                                                               \
-      cudaGetLastError();                                                                                  \
-      return fail(e_ == cudaErrorMemoryAllocation ? DNSPIR_ERR_OOM : DNSPIR_ERR_CUDA,                      \
-                  std::string(#call) + ": " + cudaGetErrorString(e_));                                     \
-    }                                                                                                      \
-  } while (0)
-#define CKR(expr)             \
-  do {                        \
-    int r_ = (expr);          \
-    if (r_ != DNSPIR_OK) return r_; \
-  } while (0)
-
 // ------------------------------------------------------------- host maths
 typedef unsigned __int128 u128;
 static uint64_t powmod(uint64_t b, uint64_t e, uint64_t p) {
@@ -61,14 +47,12 @@ static uint64_t prim_root_2n(uint64_t p, uint64_t two_n) {
     if (powmod(g, (p - 1) / 2, p) != 1) return powmod(g, (p - 1) / two_n, p);
 }
 
-namespace dnspir {
 CrtConst host_crt_const() {
   CrtConst c;
   c.q2inv1 = (uint32_t)invmod(P2 % P1, P1);
   c.q1inv2 = (uint32_t)invmod(P1 % P2, P2);
   return c;
 }
-}  // namespace dnspir
 
 // ---- seed expansion (bfv.rs:46-49).  The six a-parts are drawn from a
 // ChaCha12 word stream keyed by the 32-byte seed (rand_chacha 0.3.1 StdRng:
@@ -153,15 +137,6 @@ void expand(uint32_t n, const uint8_t* seed, uint64_t* out) {
 }  // namespace
 
 // ------------------------------------------------------------ device context
-struct DeviceCtx {
-  int device = -1;
-  uint32_t* tables = nullptr;
-  NttTables T;
-  uint32_t* consts[LOG2_N_MAX + 1] = {};  // a-parts in NTT form: [6][2][N], bit-reversed positions
-  uint32_t* galb[LOG2_N_MAX + 1] = {};
-  std::mutex mu;
-};
-
 static std::mutex g_ctx_mu;
 static DeviceCtx* g_ctx[64];
 
@@ -197,7 +172,7 @@ static int build_tables(DeviceCtx& c) {
   return DNSPIR_OK;
 }
 
-static int get_ctx(int device, DeviceCtx** out) {
+int get_ctx(int device, DeviceCtx** out) {
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
@@ -218,7 +193,7 @@ static int get_ctx(int device, DeviceCtx** out) {
 }
 
 // a-parts and the sigma_5 position map for ring dimension 2^log2n
-static int ctx_consts(DeviceCtx* c, int log2n) {
+int ctx_consts(DeviceCtx* c, int log2n) {
   std::lock_guard<std::mutex> lk(c->mu);
   if (c->consts[log2n]) return DNSPIR_OK;
   const uint32_t n = 1u << log2n;
@@ -244,6 +219,24 @@ static int ctx_consts(DeviceCtx* c, int log2n) {
     gb[pos] = brv_host((g - 1) / 2, log2n);
   }
   CK(cudaMemcpy(dg, gb.data(), n * 4, cudaMemcpyHostToDevice));
+  {
+    // (sign, e) order of the scan: position u = sign * N/2 + e <-> residue +-5^e mod 2N
+    std::vector<uint32_t> gt(n), uo(n);
+    uint32_t p5 = 1;
+    for (uint32_t e = 0; e < n / 2; e++) {
+      gt[e] = p5;
+      gt[n / 2 + e] = two_n - p5;
+      p5 = (uint32_t)(((uint64_t)p5 * 5) % two_n);
+    }
+    for (uint32_t u = 0; u < n; u++) uo[(gt[u] - 1) / 2] = u;
+    uint32_t *dgt = nullptr, *duo = nullptr;
+    CK(cudaMalloc(&dgt, n * 4));
+    CK(cudaMalloc(&duo, n * 4));
+    CK(cudaMemcpy(dgt, gt.data(), n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(duo, uo.data(), n * 4, cudaMemcpyHostToDevice));
+    c->gtab[log2n] = dgt;
+    c->uof[log2n] = duo;
+  }
   CK(cudaDeviceSynchronize());
   CK(cudaFree(dz));
   device_pow5(log2n, false);
@@ -253,38 +246,24 @@ static int ctx_consts(DeviceCtx* c, int log2n) {
   return DNSPIR_OK;
 }
 
-static ChainConsts chain_consts(DeviceCtx* c, int log2n, int used_seeds) {
+SlotMaps slot_maps(DeviceCtx* c, int log2n) {
+  SlotMaps m;
+  m.g = c->gtab[log2n];
+  m.uof = c->uof[log2n];
+  return m;
+}
+
+ChainConsts chain_consts(DeviceCtx* c, int log2n, int used_seeds) {
   const size_t n2 = (size_t)2 << log2n;
   ChainConsts cc;
   cc.gka = c->consts[log2n];
   cc.qa = c->consts[log2n] + (2 + 2 * used_seeds) * n2;
   cc.galb = c->galb[log2n];
+  cc.maps = slot_maps(c, log2n);
   return cc;
 }
 
-// RAII device buffer
-struct DBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~DBuf() {
-    if (p) cudaFree(p);
-  }
-  int ensure(size_t b) {
-    if (b <= bytes) return DNSPIR_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    CK(cudaMalloc(&p, b));
-    bytes = b;
-    return DNSPIR_OK;
-  }
-  template <class T>
-  T* as() const {
-    return (T*)p;
-  }
-};
-
-static int check_group(uint32_t log2n, uint32_t l) {
+int check_group(uint32_t log2n, uint32_t l) {
   if (log2n < 3 || log2n > LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_SHAPE, "log2_n must be in [3, 11]");
   const uint32_t n = 1u << log2n;
   if (l == 0 || n % l != 0) return fail(DNSPIR_ERR_BAD_SHAPE, "group order must divide N");
@@ -293,15 +272,9 @@ static int check_group(uint32_t log2n, uint32_t l) {
   return DNSPIR_OK;
 }
 
-// -------------------------------------------------------------- shard state
-// Device buffers shared by set_db and the secondary phase.
-struct EncodeWs {
-  DBuf A, Ahat, in16, a_out, slab_ptrs;
-};
-
 // Encodes `count` shards' entries (device u16, one shard after another) into
 // their slabs, runs the preprocessing chain and the a-part finalisation.
-static int preprocess_shards(DeviceCtx* c, const Group& g, int used_seeds, uint32_t* const* slabs_host, int count,
+int preprocess_shards(DeviceCtx* c, const Group& g, int used_seeds, uint32_t* const* slabs_host, int count,
                              const uint16_t* entries_dev, uint64_t* a_zq, uint32_t* a_ms, EncodeWs& ws,
                              cudaStream_t st) {
   const size_t per_shard = (size_t)SIMD * g.l * g.n;
@@ -312,7 +285,7 @@ static int preprocess_shards(DeviceCtx* c, const Group& g, int used_seeds, uint3
   for (int s = 0; s < count; s++) {
     launch_encode_cols(entries_dev + s * per_shard, ws.A.as<uint32_t>(), g, g.l, SIMD, c->T, st);
     launch_encode_rows(ws.A.as<uint32_t>(), ws.Ahat.as<uint32_t>(), g, g.l, SIMD, c->T, st);
-    launch_encode_lift(ws.Ahat.as<uint32_t>(), slabs_host[s], g, SIMD, 0, c->T, st);
+    launch_encode_lift(ws.Ahat.as<uint32_t>(), slabs_host[s], g, SIMD, 0, slot_maps(c, g.log2n), c->T, st);
   }
   CK(cudaMemcpyAsync(ws.slab_ptrs.p, slabs_host, (size_t)count * sizeof(uint32_t*), cudaMemcpyHostToDevice, st));
   launch_primary_chain(ws.slab_ptrs.as<uint32_t*>(), count, ws.a_out.as<uint32_t>(), g,
@@ -322,6 +295,14 @@ static int preprocess_shards(DeviceCtx* c, const Group& g, int used_seeds, uint3
   CK(cudaStreamSynchronize(st));
   return DNSPIR_OK;
 }
+
+bool reduced(const uint64_t* v, size_t n) {
+  for (size_t i = 0; i < n; i++)
+    if (v[i] >= QQ) return false;
+  return true;
+}
+
+}  // namespace dnspir
 
 struct dnspir_db {
   int device = 0;
@@ -340,78 +321,6 @@ struct dnspir_db {
   }
 };
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int d) {
-    cudaGetDevice(&prev);
-    cudaSetDevice(d);
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
-
-// RAII pinned host buffer (asynchronous copies need page-locked memory)
-struct HBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~HBuf() {
-    if (p) cudaFreeHost(p);
-  }
-  int ensure(size_t b) {
-    if (b <= bytes) return DNSPIR_OK;
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    bytes = 0;
-    CK(cudaMallocHost(&p, b));
-    bytes = b;
-    return DNSPIR_OK;
-  }
-};
-
-// ------------------------------------------------------------------ fleet
-// Buffers of one query in flight.  Two slots alternate by query parity so that
-// the primary phase of query k+1 (main stream) overlaps the secondary phase of
-// query k (secondary stream); events order the reuse of a slot.
-struct QSlot {
-  DBuf qbytes, qnat, qbrv, sec_in, reply_dev;
-  HBuf qpin;  // host staging of the query bytes
-  cudaEvent_t prim_done = nullptr, sec_done = nullptr;
-  bool sec_pending = false, prim_recorded = false;
-};
-
-struct dnspir_fleet {
-  int device = 0;
-  DeviceCtx* ctx = nullptr;
-  Group g1, g2;
-  uint32_t S = 0, D = 0;
-  cudaStream_t own = nullptr, st = nullptr, sec = nullptr;
-  std::vector<uint32_t*> slabs;
-  std::vector<bool> ready;
-  DBuf slabs_dev, distinct_dev, a_zq, a_ms;
-  EncodeWs ws;
-  QSlot slot[2];
-  DBuf part, secE, chain_out, qzq, reply_zq;  // used by one stream at a time
-  HBuf rpin;                                  // host staging of the replies of one call
-  int R = 1;
-  std::vector<cudaEvent_t> tev;  // 6 timing events per query of the last call
-  std::vector<int> tev_ok;
-  uint32_t tev_n = 0;
-  std::mutex mu;
-  ~dnspir_fleet() {
-    for (uint32_t* s : slabs)
-      if (s) cudaFree(s);
-    for (auto& e : tev)
-      if (e) cudaEventDestroy(e);
-    for (auto& s : slot) {
-      if (s.prim_done) cudaEventDestroy(s.prim_done);
-      if (s.sec_done) cudaEventDestroy(s.sec_done);
-    }
-    if (sec) cudaStreamDestroy(sec);
-    if (own) cudaStreamDestroy(own);
-  }
-};
-
 // Read-only view of a shard for the no-allocation entry point (noalloc.cu).
 namespace dnspir {
 int db_view(const dnspir_db* db, DbView* out) {
@@ -420,6 +329,7 @@ int db_view(const dnspir_db* db, DbView* out) {
   out->g = db->g;
   out->slab = db->slab;
   out->T = db->ctx->T;
+  out->maps = slot_maps(db->ctx, db->g.log2n);
   return DNSPIR_OK;
 }
 void set_last_error(const std::string& msg) { g_err = msg; }
@@ -537,12 +447,6 @@ int dnspir_db_get_a(dnspir_db* db, uint64_t* out) {
   return DNSPIR_OK;
 }
 
-static bool reduced(const uint64_t* v, size_t n) {
-  for (size_t i = 0; i < n; i++)
-    if (v[i] >= QQ) return false;
-  return true;
-}
-
 int dnspir_db_perform_pir_split(dnspir_db* db, const uint64_t* qry_b, const uint64_t* qry_conj_b, const uint64_t* gk_b,
                                 uint64_t* out_b) {
   if (!db || !qry_b || !gk_b || !out_b) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
@@ -569,8 +473,10 @@ int dnspir_db_perform_pir_split(dnspir_db* db, const uint64_t* qry_b, const uint
   CKR(db->out.ensure((size_t)SIMD * n * 8));
   CK(cudaMemcpyAsync(db->qz.p, z.data(), z.size() * 8, cudaMemcpyHostToDevice, db->st));
   launch_ring_to_ntt(db->qz.as<uint64_t>(), SIMD * 4, db->qlane.as<uint32_t>(), nullptr, g.log2n, db->ctx->T, db->st);
-  launch_scan_lanes(db->slab, db->qlane.as<uint32_t>(), db->part.as<uint32_t>(), g, R, db->st);
-  launch_epilogue_zq(db->part.as<uint32_t>(), g.H * R, db->out.as<uint64_t>(), g, db->ctx->T, db->st);
+  launch_scan_lanes(db->slab, db->qlane.as<uint32_t>(), db->part.as<uint32_t>(), g, R, slot_maps(db->ctx, g.log2n),
+                    db->st);
+  launch_epilogue_zq(db->part.as<uint32_t>(), g.H * R, db->out.as<uint64_t>(), g, slot_maps(db->ctx, g.log2n),
+                     db->ctx->T, db->st);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out_b, db->out.p, (size_t)SIMD * n * 8, cudaMemcpyDeviceToHost, db->st));
   CK(cudaStreamSynchronize(db->st));
@@ -581,392 +487,6 @@ int dnspir_db_destroy(dnspir_db* db) {
   if (!db) return DNSPIR_OK;
   DeviceGuard dg(db->device);
   delete db;
-  return DNSPIR_OK;
-}
-
-// ---------------------------------------------------------------- fleets
-int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_order, uint32_t secondary_order,
-                                uint32_t num_shards, uint32_t num_distinct, dnspir_fleet** out) {
-  if (!out) return fail(DNSPIR_ERR_BAD_ARG, "null output");
-  *out = nullptr;
-  CKR(check_group(log2_n, primary_order));
-  CKR(check_group(log2_n, secondary_order));
-  if (num_shards == 0 || num_distinct == 0 || num_distinct > num_shards)
-    return fail(DNSPIR_ERR_BAD_ARG, "need 1 <= num_distinct <= num_shards");
-  if ((uint64_t)num_shards * SIMD > secondary_order)
-    return fail(DNSPIR_ERR_BAD_SHAPE, "secondary group too small for the number of shards (double_pir.rs:152)");
-  DeviceCtx* c = nullptr;
-  CKR(get_ctx(device, &c));
-  DeviceGuard dg(device);
-  CKR(ctx_consts(c, log2_n));
-  std::unique_ptr<dnspir_fleet> f(new dnspir_fleet());
-  f->device = device;
-  f->ctx = c;
-  f->g1 = make_group(log2_n, primary_order);
-  f->g2 = make_group(log2_n, secondary_order);
-  f->S = num_shards;
-  f->D = num_distinct;
-  CK(cudaStreamCreateWithFlags(&f->own, cudaStreamNonBlocking));
-  {
-    // the secondary phase runs at the highest priority so that its few,
-    // long-lived chain blocks are dispatched ahead of pending scan blocks
-    int lo = 0, hi = 0;
-    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-    CK(cudaStreamCreateWithPriority(&f->sec, cudaStreamNonBlocking, hi));
-  }
-  f->st = f->own;
-  for (auto& s : f->slot) {
-    CK(cudaEventCreateWithFlags(&s.prim_done, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&s.sec_done, cudaEventDisableTiming));
-  }
-  f->slabs.assign(num_distinct, nullptr);
-  f->ready.assign(num_distinct, false);
-  const size_t words = slab_words(f->g1);
-  for (uint32_t d = 0; d < num_distinct; d++) CK(cudaMalloc(&f->slabs[d], words * 4));
-  std::vector<uint32_t*> ptrs(num_shards);
-  std::vector<int> dist(num_shards);
-  for (uint32_t s = 0; s < num_shards; s++) {
-    ptrs[s] = f->slabs[s % num_distinct];
-    dist[s] = (int)(s % num_distinct);
-  }
-  CKR(f->slabs_dev.ensure(num_shards * sizeof(uint32_t*)));
-  CKR(f->distinct_dev.ensure(num_shards * sizeof(int)));
-  CK(cudaMemcpy(f->slabs_dev.p, ptrs.data(), num_shards * sizeof(uint32_t*), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(f->distinct_dev.p, dist.data(), num_shards * sizeof(int), cudaMemcpyHostToDevice));
-  CKR(f->a_zq.ensure((size_t)num_distinct * SIMD * f->g1.n * 8));
-  CKR(f->a_ms.ensure((size_t)num_distinct * SIMD * f->g1.n * 4));
-  f->R = scan_chunks(f->g1, num_shards);
-  *out = f.release();
-  return DNSPIR_OK;
-}
-
-int dnspir_fleet_create(int device, uint64_t num_entries, uint32_t num_distinct, dnspir_fleet** out) {
-  uint32_t l1 = 0, l2 = 0, s = 0;
-  CKR(dnspir_get_database_shape(num_entries, &l1, &l2, &s));
-  return dnspir_fleet_create_general(device, LOG2_N_MAX, l1, l2, s, num_distinct, out);
-}
-
-int dnspir_fleet_set_shards(dnspir_fleet* f, uint32_t first, uint32_t count, const uint16_t* entries,
-                            int entries_on_device) {
-  if (!f || !entries) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
-  std::lock_guard<std::mutex> lk(f->mu);
-  if ((uint64_t)first + count > f->D) return fail(DNSPIR_ERR_BAD_ARG, "distinct shard index out of range");
-  DeviceGuard dg(f->device);
-  const size_t per = (size_t)SIMD * f->g1.l * f->g1.n;
-  const uint32_t batch = 16;
-  for (uint32_t b0 = 0; b0 < count; b0 += batch) {
-    const uint32_t cnt = count - b0 < batch ? count - b0 : batch;
-    const uint16_t* src = entries + (size_t)b0 * per;
-    if (!entries_on_device) {
-      CKR(f->ws.in16.ensure((size_t)cnt * per * 2));
-      CK(cudaMemcpyAsync(f->ws.in16.p, src, (size_t)cnt * per * 2, cudaMemcpyHostToDevice, f->st));
-      src = f->ws.in16.as<uint16_t>();
-    }
-    for (uint32_t i = 0; i < cnt; i++) f->ready[first + b0 + i] = false;
-    CKR(preprocess_shards(f->ctx, f->g1, 0, &f->slabs[first + b0], (int)cnt, src,
-                          f->a_zq.as<uint64_t>() + (size_t)(first + b0) * SIMD * f->g1.n,
-                          f->a_ms.as<uint32_t>() + (size_t)(first + b0) * SIMD * f->g1.n, f->ws, f->st));
-    for (uint32_t i = 0; i < cnt; i++) f->ready[first + b0 + i] = true;
-  }
-  return DNSPIR_OK;
-}
-
-static int fleet_ready(dnspir_fleet* f) {
-  for (uint32_t d = 0; d < f->D; d++)
-    if (!f->ready[d]) return fail(DNSPIR_ERR_NOT_READY, "fleet shard not preprocessed");
-  return DNSPIR_OK;
-}
-
-// Timing events of query i of the current call (created on demand).
-static int query_events(dnspir_fleet* f, uint32_t i, cudaEvent_t** out) {
-  while (f->tev.size() < 6 * (size_t)(i + 1)) {
-    cudaEvent_t e;
-    CK(cudaEventCreate(&e));
-    f->tev.push_back(e);
-  }
-  if (f->tev_ok.size() < (size_t)i + 1) f->tev_ok.resize(i + 1, 0);
-  *out = &f->tev[6 * (size_t)i];
-  return DNSPIR_OK;
-}
-
-static int slot_workspace(dnspir_fleet* f, QSlot& s) {
-  const uint32_t n = f->g1.n;
-  CKR(s.qnat.ensure((size_t)6 * 2 * n * 4));
-  CKR(s.qbrv.ensure((size_t)6 * 2 * n * 4));
-  CKR(s.sec_in.ensure((size_t)f->g2.l * CTXT_PARTS * n * 2));
-  return DNSPIR_OK;
-}
-
-// Primary phase of one query on the main stream: the slot's decoded vectors
-// (already written by `load`, which runs first) -> scan of every shard ->
-// epilogue into the slot's secondary entries.  Events: t[1] scan start,
-// t[2] scan end, t[3] primary end.
-static int stage_primary(dnspir_fleet* f, QSlot& s, cudaEvent_t* t) {
-  const Group& g1 = f->g1;
-  const uint32_t n = g1.n;
-  cudaStream_t st = f->st;
-  const int chunks = g1.H * f->R;
-  CKR(f->part.ensure((size_t)chunks * f->S * 2 * n * SIMD * 4));
-  if (t) CK(cudaEventRecord(t[1], st));
-  launch_scan_plain(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), f->part.as<uint32_t>(), g1, f->R, st);
-  if (t) CK(cudaEventRecord(t[2], st));
-  launch_primary_epilogue(f->part.as<uint32_t>(), chunks, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
-                          s.sec_in.as<uint16_t>(), CTXT_PARTS, 0, g1, f->ctx->T, st);
-  if (t) CK(cudaEventRecord(t[3], st));
-  CK(cudaEventRecord(s.prim_done, st));
-  s.prim_recorded = true;
-  CK(cudaGetLastError());
-  return DNSPIR_OK;
-}
-
-// Secondary phase on the secondary stream: encode the per-query database,
-// run the fused key-switch chain, write the reply (bytes, or Z_q ciphertexts),
-// and copy reply bytes to the host when host_reply is given.  Events: t[4]
-// secondary start, t[5] end.
-static int stage_secondary(dnspir_fleet* f, QSlot& s, cudaEvent_t* t, uint8_t* reply_dev, uint64_t* reply_zq,
-                           uint8_t* host_reply) {
-  const Group& g2 = f->g2;
-  const uint32_t n = g2.n;
-  cudaStream_t st = f->sec;
-  CKR(f->ws.A.ensure((size_t)g2.l * CTXT_PARTS * n * 4));
-  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * CTXT_PARTS * n * 4));
-  CKR(f->secE.ensure((size_t)2 * g2.H * g2.L * CTXT_PARTS * n * 4));
-  CKR(f->chain_out.ensure((size_t)g2.H * CTXT_PARTS * 2 * 2 * n * 4));
-  CK(cudaStreamWaitEvent(st, s.prim_done, 0));
-  if (t) CK(cudaEventRecord(t[4], st));
-  const uint32_t l_in = f->S * SIMD;
-  launch_encode_cols(s.sec_in.as<uint16_t>(), f->ws.A.as<uint32_t>(), g2, l_in, CTXT_PARTS, f->ctx->T, st);
-  launch_encode_rows(f->ws.A.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, CTXT_PARTS, f->ctx->T, st);
-  launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, CTXT_PARTS, 1, f->ctx->T, st);
-  launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>(), (size_t)6 * 2 * n, 1,
-                         f->chain_out.as<uint32_t>(), g2, chain_consts(f->ctx, g2.log2n, 1), f->ctx->T, st);
-  launch_reply(f->chain_out.as<uint32_t>(), 1, g2.H, reply_dev, 0, reply_zq, g2.log2n, f->ctx->T, st);
-  if (host_reply) CK(cudaMemcpyAsync(host_reply, reply_dev, dnspir_reply_bytes(), cudaMemcpyDeviceToHost, st));
-  if (t) CK(cudaEventRecord(t[5], st));
-  CK(cudaEventRecord(s.sec_done, st));
-  s.sec_pending = true;
-  CK(cudaGetLastError());
-  return DNSPIR_OK;
-}
-
-// Before a slot is reused, the main stream waits for the slot's previous
-// secondary phase (it reads the slot's decoded vectors and entries).
-static int slot_acquire(dnspir_fleet* f, QSlot& s) {
-  if (s.sec_pending) CK(cudaStreamWaitEvent(f->st, s.sec_done, 0));
-  s.sec_pending = false;
-  return DNSPIR_OK;
-}
-
-// End of a call: the main stream waits for every secondary phase, then the host.
-static int fleet_drain(dnspir_fleet* f) {
-  for (auto& s : f->slot)
-    if (s.sec_pending) CK(cudaStreamWaitEvent(f->st, s.sec_done, 0));
-  CK(cudaStreamSynchronize(f->st));
-  for (auto& s : f->slot) s.sec_pending = false;
-  return DNSPIR_OK;
-}
-
-static PolySpec wire_spec(const Group& g1, const Group& g2) {
-  PolySpec spec;
-  memset(&spec, 0, sizeof(spec));
-  uint32_t off = 0;
-  auto add = [&](int slot, int bits) {
-    spec.off[spec.npoly] = off;
-    spec.bits[spec.npoly] = bits;
-    spec.slot[spec.npoly] = slot;
-    spec.npoly++;
-    off += g1.n * bits / 8;
-  };
-  add(0, GK_BITS);
-  add(1, GK_BITS);
-  add(2, PQ_BITS);
-  if (g1.H == 2) add(3, PQ_BITS);
-  add(4, SQ_BITS);
-  if (g2.H == 2) add(5, SQ_BITS);
-  return spec;
-}
-
-int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries, const uint64_t* query_lens,
-                                 uint32_t nq, uint8_t* replies, uint64_t reply_stride, int32_t* status,
-                                 int on_device) {
-  if (!f || (!queries && nq) || (!query_lens && nq) || (!replies && nq)) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
-  if (nq && reply_stride < dnspir_reply_bytes()) return fail(DNSPIR_ERR_BAD_ARG, "reply stride too small");
-  std::lock_guard<std::mutex> lk(f->mu);
-  CKR(fleet_ready(f));
-  const Group& g1 = f->g1;
-  const Group& g2 = f->g2;
-  if (g1.log2n != LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_SHAPE, "the wire format is defined for N = 2048");
-  DeviceGuard dg(f->device);
-  const uint64_t want = dnspir_query_bytes(g1.l, g2.l);
-  const PolySpec spec = wire_spec(g1, g2);
-  f->tev_n = 0;
-  std::fill(f->tev_ok.begin(), f->tev_ok.end(), 0);
-  const size_t RB = dnspir_reply_bytes();
-  if (!on_device) CKR(f->rpin.ensure((size_t)nq * RB));
-  int first_err = DNSPIR_OK;
-  std::string first_msg;
-  uint32_t k = 0;  // answered queries so far (slot parity)
-  for (uint32_t i = 0; i < nq; i++) {
-    int r = DNSPIR_OK;
-    if (!queries[i]) r = fail(DNSPIR_ERR_BAD_ARG, "null query");
-    else if (query_lens[i] != want) r = fail(DNSPIR_ERR_BAD_SIZE, "query length does not match the database shape");
-    cudaEvent_t* t = nullptr;
-    if (r == DNSPIR_OK) r = query_events(f, i, &t);
-    if (r == DNSPIR_OK) {
-      QSlot& s = f->slot[k & 1];
-      r = slot_acquire(f, s);
-      if (r == DNSPIR_OK) r = slot_workspace(f, s);
-      if (r == DNSPIR_OK && !on_device) {
-        r = s.qbytes.ensure(want);
-        if (r == DNSPIR_OK) r = s.qpin.ensure(want);
-        if (r == DNSPIR_OK) r = s.reply_dev.ensure(RB);
-        // the slot's staging buffer may still feed the copy of the query two back
-        if (r == DNSPIR_OK && s.prim_recorded && cudaEventSynchronize(s.prim_done) != cudaSuccess)
-          r = fail(DNSPIR_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
-        if (r == DNSPIR_OK) memcpy(s.qpin.p, queries[i], want);
-      }
-      if (r == DNSPIR_OK) {
-        cudaError_t e = cudaEventRecord(t[0], f->st);
-        const uint8_t* src = queries[i];
-        if (e == cudaSuccess && !on_device) {
-          e = cudaMemcpyAsync(s.qbytes.p, s.qpin.p, want, cudaMemcpyHostToDevice, f->st);
-          src = s.qbytes.as<uint8_t>();
-        }
-        if (e != cudaSuccess) r = fail(DNSPIR_ERR_CUDA, cudaGetErrorString(e));
-        else launch_decode_query(src, spec, s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), g1.log2n, f->ctx->T, f->st);
-      }
-      if (r == DNSPIR_OK) r = stage_primary(f, s, t);
-      if (r == DNSPIR_OK)
-        r = on_device ? stage_secondary(f, s, t, replies + (size_t)i * reply_stride, nullptr, nullptr)
-                      : stage_secondary(f, s, t, s.reply_dev.as<uint8_t>(), nullptr, (uint8_t*)f->rpin.p + i * RB);
-      if (r == DNSPIR_OK) k++;
-      f->tev_ok[i] = r == DNSPIR_OK;
-      f->tev_n = i + 1;
-    }
-    if (status) status[i] = r;
-    if (r == DNSPIR_ERR_CUDA || r == DNSPIR_ERR_OOM) return r;
-    if (r != DNSPIR_OK && first_err == DNSPIR_OK) {
-      first_err = r;
-      first_msg = g_err;
-    }
-  }
-  CKR(fleet_drain(f));
-  if (!on_device)
-    for (uint32_t i = 0; i < nq; i++)
-      if (i < f->tev_ok.size() && f->tev_ok[i] && i < f->tev_n)
-        memcpy(replies + (size_t)i * reply_stride, (uint8_t*)f->rpin.p + i * RB, RB);
-  if (first_err != DNSPIR_OK) g_err = first_msg;
-  return first_err;
-}
-
-int dnspir_fleet_process_query(dnspir_fleet* f, const uint8_t* query, uint64_t query_len, uint8_t* reply,
-                               uint64_t* reply_len) {
-  int32_t st = 0;
-  const uint8_t* qs[1] = {query};
-  uint64_t ls[1] = {query_len};
-  CKR(dnspir_fleet_process_queries(f, qs, ls, 1, reply, dnspir_reply_bytes(), &st, 0));
-  if (reply_len) *reply_len = dnspir_reply_bytes();
-  return DNSPIR_OK;
-}
-
-int dnspir_fleet_perform_double_pir(dnspir_fleet* f, const uint64_t* pq, const uint64_t* pqc, const uint64_t* sq,
-                                    const uint64_t* sqc, const uint64_t* gk, uint64_t* out) {
-  if (!f || !pq || !sq || !gk || !out) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
-  std::lock_guard<std::mutex> lk(f->mu);
-  CKR(fleet_ready(f));
-  if ((f->g1.H == 2) != (pqc != nullptr))
-    return fail(DNSPIR_ERR_BAD_SHAPE, "conjugate primary query must be given exactly when required (double_pir.rs:160)");
-  if ((f->g2.H == 2) != (sqc != nullptr))
-    return fail(DNSPIR_ERR_BAD_SHAPE, "conjugate secondary query must be given exactly when required");
-  const size_t n = f->g1.n;
-  std::vector<uint64_t> z(6 * n, 0);
-  memcpy(&z[0], gk, n * 8);
-  memcpy(&z[n], gk + n, n * 8);
-  memcpy(&z[2 * n], pq, n * 8);
-  if (pqc) memcpy(&z[3 * n], pqc, n * 8);
-  memcpy(&z[4 * n], sq, n * 8);
-  if (sqc) memcpy(&z[5 * n], sqc, n * 8);
-  if (!reduced(z.data(), z.size())) return fail(DNSPIR_ERR_BAD_ARG, "ring element coefficients must be below q");
-  DeviceGuard dg(f->device);
-  QSlot& s = f->slot[0];
-  cudaEvent_t* t = nullptr;
-  CKR(query_events(f, 0, &t));
-  CKR(slot_acquire(f, s));
-  CKR(slot_workspace(f, s));
-  CKR(f->qzq.ensure(z.size() * 8));
-  CKR(f->reply_zq.ensure((size_t)CTXT_PARTS * 2 * n * 8));
-  CK(cudaEventRecord(t[0], f->st));
-  CK(cudaMemcpyAsync(f->qzq.p, z.data(), z.size() * 8, cudaMemcpyHostToDevice, f->st));
-  launch_ring_to_ntt(f->qzq.as<uint64_t>(), 6, s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), f->g1.log2n, f->ctx->T,
-                     f->st);
-  CKR(stage_primary(f, s, t));
-  CKR(stage_secondary(f, s, t, nullptr, f->reply_zq.as<uint64_t>(), nullptr));
-  f->tev_ok[0] = 1;
-  f->tev_n = 1;
-  CKR(fleet_drain(f));
-  CK(cudaMemcpy(out, f->reply_zq.p, (size_t)CTXT_PARTS * 2 * n * 8, cudaMemcpyDeviceToHost));
-  return DNSPIR_OK;
-}
-
-int dnspir_fleet_batch_timings(dnspir_fleet* f, uint32_t max, double* latency_ms, double* primary_ms,
-                               double* secondary_ms, double* scan_ms) {
-  if (!f) return -fail(DNSPIR_ERR_BAD_ARG, "null fleet");
-  std::lock_guard<std::mutex> lk(f->mu);
-  DeviceGuard dg(f->device);
-  const uint32_t n = f->tev_n < max ? f->tev_n : max;
-  for (uint32_t i = 0; i < n; i++) {
-    double v[4] = {-1, -1, -1, -1};
-    if (f->tev_ok[i]) {
-      cudaEvent_t* t = &f->tev[6 * (size_t)i];
-      float a = 0, b = 0, c = 0, d = 0;
-      if (cudaEventSynchronize(t[5]) != cudaSuccess || cudaEventElapsedTime(&a, t[0], t[5]) != cudaSuccess ||
-          cudaEventElapsedTime(&b, t[0], t[3]) != cudaSuccess || cudaEventElapsedTime(&c, t[4], t[5]) != cudaSuccess ||
-          cudaEventElapsedTime(&d, t[1], t[2]) != cudaSuccess) {
-        cudaGetLastError();
-        return -fail(DNSPIR_ERR_CUDA, "timing events unavailable");
-      }
-      v[0] = a, v[1] = b, v[2] = c, v[3] = d;
-    }
-    if (latency_ms) latency_ms[i] = v[0];
-    if (primary_ms) primary_ms[i] = v[1];
-    if (secondary_ms) secondary_ms[i] = v[2];
-    if (scan_ms) scan_ms[i] = v[3];
-  }
-  return (int)n;
-}
-
-int dnspir_fleet_last_timings(dnspir_fleet* f, double* primary_ms, double* secondary_ms, double* scan_ms) {
-  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
-  uint32_t n = 0;
-  {
-    std::lock_guard<std::mutex> lk(f->mu);
-    n = f->tev_n;
-    if (!n || !f->tev_ok[n - 1]) return fail(DNSPIR_ERR_NOT_READY, "no query answered yet");
-  }
-  std::vector<double> p(n), s(n), c(n);
-  const int got = dnspir_fleet_batch_timings(f, n, nullptr, p.data(), s.data(), c.data());
-  if (got < 0) return -got;
-  if (primary_ms) *primary_ms = p[n - 1];
-  if (secondary_ms) *secondary_ms = s[n - 1];
-  if (scan_ms) *scan_ms = c[n - 1];
-  return DNSPIR_OK;
-}
-
-int dnspir_fleet_set_stream(dnspir_fleet* f, void* s) {
-  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
-  std::lock_guard<std::mutex> lk(f->mu);
-  f->st = s ? (cudaStream_t)s : f->own;
-  return DNSPIR_OK;
-}
-
-uint64_t dnspir_fleet_slab_bytes(dnspir_fleet* f) { return f ? (uint64_t)f->D * slab_words(f->g1) * 4 : 0; }
-
-int dnspir_fleet_destroy(dnspir_fleet* f) {
-  if (!f) return DNSPIR_OK;
-  DeviceGuard dg(f->device);
-  cudaStreamSynchronize(f->st);
-  cudaStreamSynchronize(f->sec);
-  delete f;
   return DNSPIR_OK;
 }
 

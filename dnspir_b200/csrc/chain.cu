@@ -173,6 +173,7 @@ struct ChainArgs {
   const uint32_t* gka;
   const uint32_t* qa;
   const uint32_t* galb;
+  SlotMaps maps;
   NttTables T;
   ChainPrime cp[2];
   // secondary: entries in chain layout, query vectors [q][slot][p][pos], output
@@ -253,7 +254,7 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
         } else {
           const uint32_t j = brv(pos, logn);
           const uint32_t ks = gidx(cinv * (2 * j + 1), mask);
-          e[c] = slab[slab_off(a.g, p, h, i, 0, ks) + lane];
+          e[c] = slab[slab_off(a.g, p, h, i, 0, __ldg(a.maps.uof + ks)) + lane];
         }
       }
     }
@@ -310,11 +311,12 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
     }
     __syncthreads();
     if (!SECONDARY) {
-      // key digits of row i in the scan layout: G'[i][k] = G_i[idx(5^(L-1-i) (2k+1))]
-      for (int k = threadIdx.x; k < N; k += CT) {
-        const uint32_t jb = brv(gidx(ci * (2 * k + 1), mask), logn);
-        slab[slab_off(a.g, p, h, i, 1, k) + lane] = TC[jb];
-        slab[slab_off(a.g, p, h, i, 2, k) + lane] = D[jb];
+      // key digits of row i in the scan layout: position u (natural slot k with
+      // 2k+1 = g[u]) holds G_i[idx(5^(L-1-i) g[u])]
+      for (int u = threadIdx.x; u < N; u += CT) {
+        const uint32_t jb = brv(gidx(ci * __ldg(a.maps.g + u), mask), logn);
+        slab[slab_off(a.g, p, h, i, 1, u) + lane] = TC[jb];
+        slab[slab_off(a.g, p, h, i, 2, u) + lane] = D[jb];
       }
       // TC and D are rewritten only after the next step's first barrier
       ci = (ci * a.inv5) & mask;
@@ -403,6 +405,7 @@ static ChainArgs chain_args(const Group& g, const ChainConsts& cc, const NttTabl
   a.gka = cc.gka;
   a.qa = cc.qa;
   a.galb = cc.galb;
+  a.maps = cc.maps;
   a.T = T;
   const uint64_t n = g.n;
   const CrtConst crtc = host_crt_const();

@@ -85,7 +85,8 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
 
 // One block: column r of half h for up to 8 lanes.
 __global__ void encode_lift_kernel(const uint32_t* __restrict__ Ahat, uint32_t* __restrict__ out, Group g, int nl,
-                                   int frame, uint32_t scale, const uint32_t* __restrict__ pow5inv, NttTables T) {
+                                   int frame, uint32_t scale, const uint32_t* __restrict__ pow5inv,
+                                   const uint32_t* __restrict__ gtab, NttTables T) {
   extern __shared__ uint32_t sm[];
   const uint32_t r = blockIdx.x, h = blockIdx.y;
   const int lane0 = blockIdx.z * 8;
@@ -114,12 +115,13 @@ __global__ void encode_lift_kernel(const uint32_t* __restrict__ Ahat, uint32_t* 
   ntt_fwd_smem2(sm, logn, nlg, nlg, T);
   const uint32_t c = g.L - 1 - r;
   if (frame == 0) {
-    // scan layout: 8 lanes interleaved, natural slot order
+    // scan layout: 8 lanes interleaved, (sign, e) position u holds natural slot (g[u]-1)/2
     for (uint32_t b = threadIdx.x; b < 2 * N * SIMD; b += blockDim.x) {
       const uint32_t p = b / (N * SIMD);
       const uint32_t rem = b % (N * SIMD);
       const uint32_t u = rem / SIMD, kk = rem % SIMD;
-      out[slab_off(g, p, h, c, 0, u) + kk] = sm[((p * nlg + kk) << logn) + brv(u, logn)];
+      const uint32_t k = (__ldg(gtab + u) - 1) >> 1;
+      out[slab_off(g, p, h, c, 0, u) + kk] = sm[((p * nlg + kk) << logn) + brv(k, logn)];
     }
   } else {
     // chain layout, bit-reversed positions, E_c[j] = E^_r[idx(5^-r (2j+1))]
@@ -207,8 +209,8 @@ void launch_encode_rows(const uint32_t* A, uint32_t* Ahat, const Group& g, uint3
   encode_rows_kernel<<<grid, 256, smem, st>>>(A, Ahat, g, l_in, nl, U, logn2, pow_table(g.log2n, false), T);
 }
 
-void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int nl, int frame, const NttTables& T,
-                        cudaStream_t st) {
+void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int nl, int frame, const SlotMaps& maps,
+                        const NttTables& T, cudaStream_t st) {
   uint32_t linv = 1;
   for (uint32_t x = 1; x < TPLAIN; x++)
     if ((x * (g.l % TPLAIN)) % TPLAIN == 1) linv = x;
@@ -216,7 +218,7 @@ void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int
   const size_t smem = (size_t)2 * nlg * g.n * 4;
   dim3 grid(g.L, g.H, (nl + 7) / 8);
   set_smem(encode_lift_kernel, smem);
-  encode_lift_kernel<<<grid, 512, smem, st>>>(Ahat, out, g, nl, frame, linv, pow_table(g.log2n, true), T);
+  encode_lift_kernel<<<grid, 512, smem, st>>>(Ahat, out, g, nl, frame, linv, pow_table(g.log2n, true), maps.g, T);
 }
 
 void launch_pack_bytes(const uint8_t* bytes, uint16_t* coeffs, size_t entries, int log2n, cudaStream_t st) {

@@ -25,8 +25,16 @@ struct Group {
 };
 Group make_group(int log2n, uint32_t l);
 
+// Output slots of the scan are ordered by (sign, e): position u = sign * N/2 + e
+// holds the slot k with 2k + 1 = (sign ? -1 : 1) 5^e mod 2N.  g[u] is that odd
+// residue and uof[k] the position of natural slot k (device tables per N).
+struct SlotMaps {
+  const uint32_t* g;
+  const uint32_t* uof;
+};
+
 // Scan-layout offset (in u32 words) of array a (0 = entries E, 1/2 = key digits
-// G0/G1) of row i, half h, factor p, output slot k, lane 0 inside one shard slab.
+// G0/G1) of row i, half h, factor p, output position u, lane 0 inside one shard slab.
 __host__ __device__ __forceinline__ size_t slab_off(const Group& g, int p, int h, uint32_t i, int a, uint32_t k) {
   return (((((size_t)p * g.H + h) * g.L + i) * 3 + a) * g.n + k) * SIMD;
 }
@@ -41,14 +49,15 @@ void launch_encode_rows(const uint32_t* A, uint32_t* Ahat, const Group& g, uint3
                         cudaStream_t st);
 // Ahat -> transformed entries.  frame 0: scan layout in `slab` (nl == 8);
 // frame 1: chain layout out[((p*H + h)*L + c)*nl + lane][pos] in bit-reversed slot order.
-void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int nl, int frame, const NttTables& T,
-                        cudaStream_t st);
+void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int nl, int frame, const SlotMaps& maps,
+                        const NttTables& T, cudaStream_t st);
 
 // ---- key-switch chain (preprocess / partial_gal, base_pir.rs:496-594, 782-863)
 struct ChainConsts {
   const uint32_t* gka;    // [digit][p][pos]  (bit-reversed slot order)
   const uint32_t* qa;     // [half][p][pos]   (qry_a for the database's seed set)
   const uint32_t* galb;   // [pos] -> destination position of sigma_5 (bit-reversed coordinates)
+  SlotMaps maps;          // scan-layout slot order
 };
 // Primary preprocessing chain for `nshards` shards (slabs[s] already hold E);
 // writes G0/G1 into the slabs and a_out[s][h][lane][p][pos].
@@ -68,22 +77,26 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
                             const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st);
 
 // ---- primary scan (main_pir_loop, base_pir.rs:1085-1247)
-// qnat: [p][4][N] natural-order vectors (0 qry, 1 qry_conj, 2 gk0, 3 gk1), one query for all lanes.
-// part: [chunk][s][p][k][lane] partial sums reduced mod p.
+// B queries (B in {1, 2, 4, 8, 16}) per pass over all shards.  qnat: per query
+// [slot][p][N] natural order (slots 0 gk0, 1 gk1, 2 pq, 3 pqc), q_stride words
+// apart.  out: [b][s][p][u][lane] reduced mod p.  counter: one device word.
+int scan_batch_supported(int B);
+int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int B,
+                      uint32_t* out, const Group& g, const SlotMaps& maps, uint32_t* counter, cudaStream_t st);
+// Per-lane queries (perform_pir_split): qlane [(lane*4 + v)*2 + p][N] natural order;
+// part: [chunk][p][u][lane], chunks = H * R.
 int scan_chunks(const Group& g, int nshards);
-void launch_scan_plain(uint32_t* const* slabs_dev, int nshards, const uint32_t* qnat, uint32_t* part, const Group& g,
-                       int chunks, cudaStream_t st);
-// Per-lane queries (perform_pir_split): qlane [p][4][N][lane] natural order.
-void launch_scan_lanes(const uint32_t* slab, const uint32_t* qlane, uint32_t* part, const Group& g, int chunks,
-                       cudaStream_t st);
-// Primary epilogue: partials -> b (iNTT, CRT), mod-switch, combine with the
-// shard's a-part, three base-1025 digits -> secondary entries [t = s*8+lane][part][n].
-void launch_primary_epilogue(const uint32_t* part, int chunks, int nshards, const uint32_t* a_ms,
-                             const int* distinct_of, uint16_t* sec_in, int sec_lanes, int sec_lane0, const Group& g,
-                             const NttTables& T, cudaStream_t st);
+void launch_scan_lanes(const uint32_t* slab, const uint32_t* qlane, uint32_t* part, const Group& g, int R,
+                       const SlotMaps& maps, cudaStream_t st);
+// Primary epilogue for nq queries: scan output -> b (iNTT, CRT), mod-switch,
+// combine with the shard's a-part, three base-1025 digits -> secondary
+// entries sec_in[t = s*8+lane][q*3 + part][n].
+void launch_primary_epilogue(const uint32_t* fin, int nq, int nshards, const uint32_t* a_ms, const int* distinct_of,
+                             uint16_t* sec_in, const Group& g, const SlotMaps& maps, const NttTables& T,
+                             cudaStream_t st);
 // Epilogue returning b as Z_q coefficients [lane][n] (shard-level perform_pir_split).
-void launch_epilogue_zq(const uint32_t* part, int chunks, uint64_t* out, const Group& g, const NttTables& T,
-                        cudaStream_t st);
+void launch_epilogue_zq(const uint32_t* part, int chunks, uint64_t* out, const Group& g, const SlotMaps& maps,
+                        const NttTables& T, cudaStream_t st);
 
 // ---- wire codec (pir_wrapper.rs:84-158, 370-408)
 // Decodes one query's polynomials: poly_off/poly_bits per polynomial (npoly),
@@ -113,6 +126,7 @@ struct DbView {
   Group g;
   const uint32_t* slab;
   NttTables T;
+  SlotMaps maps;
 };
 
 // Payload helpers for synthetic databases (dns/bucket.rs:289-303 packing).

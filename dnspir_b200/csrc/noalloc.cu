@@ -123,8 +123,8 @@ extern "C" int dnspir_db_perform_pir_split_noalloc(dnspir_db* db, const uint64_t
       e = cudaMemcpy2DAsync((char*)zq + 2 * row, pitch, gk_b, 2 * row, 2 * row, SIMD, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) {
       launch_ring_to_ntt(zq, SIMD * 4, ntt, nullptr, g.log2n, v.T, st);
-      launch_scan_lanes(v.slab, ntt, part, g, chunks, st);
-      launch_epilogue_zq(part, g.H * chunks, out_b, g, v.T, st);
+      launch_scan_lanes(v.slab, ntt, part, g, chunks, v.maps, st);
+      launch_epilogue_zq(part, g.H * chunks, out_b, g, v.maps, v.T, st);
       e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

@@ -107,6 +107,10 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
  * dns/server.rs:707-728).  entries: count x (8 primary_order N) coefficients. */
 int dnspir_fleet_set_shards(dnspir_fleet* fleet, uint32_t first_distinct, uint32_t count, const uint16_t* entries,
                             int entries_on_device);
+/* Queries answered per pass over the shard slabs (1, 2, 4, 8 or 16; default
+ * 1).  dnspir_fleet_process_queries splits its queries into groups of this
+ * size; every group reads each slab once.  Replies do not depend on it. */
+int dnspir_fleet_set_batch(dnspir_fleet* fleet, uint32_t max_batch);
 /* Synthetic 2560-byte payloads packed into 10-bit coefficients
  * (pack_bytes_into_coeffs, dns/bucket.rs:289-303): bytes = entries x 2560 on
  * the device, coeffs = entries x 2048 on the device. */

@@ -171,3 +171,52 @@ def test_conjugate_presence_is_checked():
     with pytest.raises(dp.DnspirError) as e:
         fleet.perform_double_pir(z, None, z, z, np.zeros((2, 256), dtype=np.uint64))
     assert e.value.code == 2
+
+
+@pytest.mark.parametrize("batch", [2, 4, 8, 16])
+def test_batched_answers_equal_oracle(config1, batch):
+    # one pass over the slabs per group of `batch` queries; every reply must be
+    # the oracle's bytes (process_queries, pir_wrapper.rs:349)
+    data, refs, fleet, l1, l2, shards = config1
+    rng = orc.Rng(bytes([3, batch]) + bytes(30))
+    qs = [orc.prepare_query(rng, (977 * k) % 8192, k % shards, l1, l2) for k in range(batch + 2)]
+    fleet.set_batch(batch)
+    try:
+        got = fleet.process_queries([q for q, _ in qs])
+    finally:
+        fleet.set_batch(1)
+    for k, ((q, seed), r) in enumerate(zip(qs, got)):
+        assert r == orc.process_query(refs, q), k
+        i, j = (977 * k) % 8192, k % shards
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64))
+
+
+def test_batched_group_with_rejected_query(config1):
+    data, refs, fleet, l1, l2, shards = config1
+    rng = orc.Rng(bytes([4]) + bytes(31))
+    qs = [orc.prepare_query(rng, 5 * k, k % shards, l1, l2) for k in range(4)]
+    queries = [qs[0][0], qs[1][0][:-3], qs[2][0], qs[3][0]]
+    fleet.set_batch(4)
+    try:
+        with pytest.raises(dp.DnspirError) as e:
+            fleet.process_queries(queries)
+        assert e.value.code == 1
+    finally:
+        fleet.set_batch(1)
+    # the valid queries are still answered correctly in the same call
+    import ctypes
+    L = dp.lib()
+    bufs = [np.frombuffer(q, dtype=np.uint8) for q in queries]
+    ptrs = (ctypes.c_void_p * 4)(*[b.ctypes.data for b in bufs])
+    lens = (ctypes.c_uint64 * 4)(*[len(b) for b in bufs])
+    out = np.zeros((4, dp.reply_bytes()), dtype=np.uint8)
+    status = np.zeros(4, dtype=np.int32)
+    fleet.set_batch(4)
+    try:
+        rc = L.dnspir_fleet_process_queries(fleet._h, ptrs, lens, 4, out.ctypes.data_as(ctypes.c_void_p),
+                                            dp.reply_bytes(), status.ctypes.data_as(ctypes.c_void_p), 0)
+    finally:
+        fleet.set_batch(1)
+    assert rc == 1 and list(status) == [0, 1, 0, 0]
+    for k in (0, 2, 3):
+        assert out[k].tobytes() == orc.process_query(refs, queries[k])
