@@ -85,6 +85,10 @@ def lib():
         L.dnspir_fleet_last_timings.argtypes = [_vp] + [c.POINTER(c.c_double)] * 3
         L.dnspir_fleet_set_stream.argtypes = [_vp, _vp]
         L.dnspir_fleet_set_batch.argtypes = [_vp, c.c_uint32]
+        L.dnspir_fleet_set_engine.argtypes = [_vp, c.c_int]
+        L.dnspir_fleet_tune.argtypes = [_vp, c.c_uint32, _vp, _vp]
+        L.dnspir_tscan_shapes.argtypes = [_vp, _vp, _vp, c.c_int]
+        L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
         L.dnspir_fleet_batch_timings.argtypes = [_vp, c.c_uint32] + [_vp] * 4
         L.dnspir_fleet_slab_bytes.restype = c.c_uint64
         L.dnspir_fleet_slab_bytes.argtypes = [_vp]
@@ -236,6 +240,18 @@ class PIRDatabase:
                                       _zq(np.asarray(gk_b, dtype=np.uint64)[None], (8, 2, n)))
 
 
+ENGINE_CUDA_CORES = 0
+ENGINE_TENSOR = 1
+
+
+def tscan_shapes():
+    """The tensor scan's tile shapes: (query-operand rows, m-tiles, stages) per CTA."""
+    n = lib().dnspir_tscan_shapes(None, None, None, 0)
+    a = [np.zeros(n, dtype=np.int32) for _ in range(3)]
+    lib().dnspir_tscan_shapes(*[_ptr(x) for x in a], n)
+    return [tuple(int(x[i]) for x in a) for i in range(n)]
+
+
 class Fleet:
     """The primary shards of one database plus the two-level answer path.
 
@@ -345,8 +361,27 @@ class Fleet:
         return out[:, :n]
 
     def set_batch(self, max_batch):
-        """Queries per pass over the slabs (1, 2, 4, 8, 16); replies do not depend on it."""
+        """Queries per pass over the slabs (CUDA cores: 1, 2, 4, 8, 16; tensor
+        cores: 1..256); replies do not depend on it."""
         _check(lib().dnspir_fleet_set_batch(self._h, max_batch))
+
+    def scan(self, qnat, out):
+        """Primary scan alone (torch cuda tensors): qnat uint32-as-int32
+        [nq][6][2][N] natural NTT order, out [nq][shards][2][N][8]."""
+        _check(lib().dnspir_fleet_scan(self._h, _dev_ptr(qnat), qnat.shape[0], _dev_ptr(out)))
+
+    def set_engine(self, engine):
+        """ENGINE_CUDA_CORES or ENGINE_TENSOR; marks every shard unprepared."""
+        _check(lib().dnspir_fleet_set_engine(self._h, engine))
+
+    def tune(self, batch):
+        """Tensor engine: time each tile shape for groups of `batch` queries and
+        keep the fastest.  Returns (chosen index, ms per shape, shapes)."""
+        shapes = tscan_shapes()
+        ms = np.full(len(shapes), -1.0)
+        chosen = ctypes.c_int(-1)
+        _check(lib().dnspir_fleet_tune(self._h, batch, _ptr(ms), ctypes.byref(chosen)))
+        return chosen.value, ms, shapes
 
     def set_stream(self, stream_handle):
         _check(lib().dnspir_fleet_set_stream(self._h, _vp(stream_handle) if stream_handle else None))

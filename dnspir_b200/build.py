@@ -5,7 +5,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = ["api.cu", "fleet.cu", "encode.cu", "chain.cu", "scan.cu", "wire.cu", "client.cpp", "noalloc.cu"]
+SRC = ["api.cu", "fleet.cu", "encode.cu", "chain.cu", "scan.cu", "tscan.cu", "wire.cu", "client.cpp", "noalloc.cu"]
 OUT = os.path.join(HERE, "libdnspir_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -2,14 +2,18 @@
 // (perform_batched_double_pir, crates/pir/src/double_pir.rs:126-228;
 // process_queries, pir_wrapper.rs:349-409).
 //
-// Queries are answered in groups of up to `batch` (1, 2, 4, 8 or 16): one pass
-// of the scan over every shard serves the whole group (the slab is read once
-// per group), then each query's secondary database is encoded and evaluated.
+// Queries are answered in groups of up to `batch`: one pass of the scan over
+// every shard serves the whole group (the slab is read once per group), then
+// the secondary databases are encoded and evaluated in chunks of up to 16
+// queries.  Two scan engines: CUDA cores over the lane layout (groups of 1, 2,
+// 4, 8 or 16) and the tensor cores over the tensor layout (groups up to 256,
+// tile shape per group size from a table or from dnspir_fleet_tune).
 // Two buffer slots alternate between groups: the primary phase of group k+1
 // (main stream) runs while the secondary phase of group k runs on a second,
 // high-priority stream; events order the reuse of a slot.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -37,12 +41,15 @@ struct dnspir_fleet {
   cudaStream_t own = nullptr, st = nullptr, sec = nullptr;
   std::vector<uint32_t*> slabs;
   std::vector<bool> ready;
-  DBuf slabs_dev, distinct_dev, a_zq, a_ms, counter;
+  DBuf slabs_dev, distinct_dev, a_zq, a_ms;
   EncodeWs ws;
   QSlot slot[2];
   DBuf secE, chain_out, qzq, reply_zq;  // used by one stream at a time
   HBuf rpin;                            // host staging of the replies of one call
   int batch = 1;
+  int engine = DNSPIR_ENGINE_CUDA_CORES;
+  DBuf qb, err_word, tmp_lane;      // tensor engine: query operand, wait-error word, preprocessing scratch
+  std::map<int, int> tuned;         // tensor engine: group size -> tile shape index
   std::vector<cudaEvent_t> tev;  // 6 timing events per group of the last call
   std::vector<int> q_group;      // per query of the last call: its group, or -1
   std::mutex mu;
@@ -63,6 +70,29 @@ struct dnspir_fleet {
 namespace {
 
 const size_t QV_WORDS_PER_QUERY = 6 * 2;  // decoded slots x factors, times N
+const int SEC_CHUNK = 16;                 // queries per secondary launch sequence
+const int TENSOR_MAX_BATCH = 256;
+
+// Tile shape of the tensor scan for a group of nb queries, and the padded
+// group size it implies.
+const TScanShape& tensor_shape(dnspir_fleet* f, int nb, int* nb_pad) {
+  int count = 0;
+  const TScanShape* sh = tscan_shapes(&count);
+  int idx;
+  auto it = f->tuned.find(nb);
+  if (it != f->tuned.end()) {
+    idx = it->second;
+  } else {
+    // untuned: the narrowest query tile that holds the group, one m-tile
+    const int want = nb <= 4 ? 16 : nb <= 8 ? 32 : nb <= 16 ? 64 : nb <= 32 ? 128 : 256;
+    idx = 0;
+    for (int i = count - 1; i >= 0; i--)
+      if (sh[i].nq == want && sh[i].mtpc == 1) idx = i;
+  }
+  const int q = sh[idx].nq / 4;
+  *nb_pad = (nb + q - 1) / q * q;
+  return sh[idx];
+}
 
 int fleet_ready(dnspir_fleet* f) {
   for (uint32_t d = 0; d < f->D; d++)
@@ -98,6 +128,7 @@ int slot_workspace(dnspir_fleet* f, QSlot& s, int Bk, int nb) {
   CKR(s.qbrv.ensure((size_t)Bk * QV_WORDS_PER_QUERY * n * 4));
   CKR(s.fin.ensure((size_t)Bk * f->S * 2 * n * SIMD * 4));
   CKR(s.sec_in.ensure((size_t)f->g2.l * CTXT_PARTS * nb * n * 2));
+  if (f->engine == DNSPIR_ENGINE_TENSOR) CKR(f->qb.ensure(tscan_query_bytes(f->g1, Bk)));
   return DNSPIR_OK;
 }
 
@@ -108,16 +139,25 @@ int stage_primary(dnspir_fleet* f, QSlot& s, int nb, int Bk, cudaEvent_t* t) {
   const Group& g1 = f->g1;
   const size_t n = g1.n;
   cudaStream_t st = f->st;
-  if (Bk > nb)  // unused query positions of the kernel batch compute on zeros
+  if (Bk > nb && f->engine == DNSPIR_ENGINE_CUDA_CORES)  // unused query positions compute on zeros
     CK(cudaMemsetAsync(s.qnat.as<uint32_t>() + (size_t)nb * QV_WORDS_PER_QUERY * n, 0,
                        (size_t)(Bk - nb) * QV_WORDS_PER_QUERY * n * 4, st));
   CK(cudaEventRecord(t[1], st));
-  if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, Bk,
-                        s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), f->counter.as<uint32_t>(), st))
+  if (f->engine == DNSPIR_ENGINE_TENSOR) {
+    int nb_pad = 0;
+    const TScanShape& shape = tensor_shape(f, nb, &nb_pad);
+    if (nb_pad != Bk) return fail(DNSPIR_ERR_BAD_ARG, "tensor scan batch mismatch");
+    if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, nb, Bk,
+                     f->qb.as<uint8_t>(), s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1,
+                     slot_maps(f->ctx, g1.log2n), shape, st))
+      return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
+  } else if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, Bk,
+                               s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), st)) {
     return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
+  }
   CK(cudaEventRecord(t[2], st));
   launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
-                          s.sec_in.as<uint16_t>(), g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, st);
+                          s.sec_in.as<uint16_t>(), SEC_CHUNK, g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, st);
   CK(cudaEventRecord(t[3], st));
   CK(cudaEventRecord(s.prim_done, st));
   s.prim_recorded = true;
@@ -133,22 +173,31 @@ int stage_secondary(dnspir_fleet* f, QSlot& s, int nb, cudaEvent_t* t, uint8_t* 
                     uint64_t* reply_zq, uint8_t* host_reply) {
   const Group& g2 = f->g2;
   const size_t n = g2.n;
-  const int nl = CTXT_PARTS * nb;
+  const int cmax = std::min(nb, SEC_CHUNK);
+  const int nlmax = CTXT_PARTS * cmax;
   cudaStream_t st = f->sec;
-  CKR(f->ws.A.ensure((size_t)g2.l * nl * n * 4));
-  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * nl * n * 4));
-  CKR(f->secE.ensure((size_t)2 * g2.H * g2.L * nl * n * 4));
-  CKR(f->chain_out.ensure((size_t)nb * g2.H * CTXT_PARTS * 2 * 2 * n * 4));
+  CKR(f->ws.A.ensure((size_t)g2.l * nlmax * n * 4));
+  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * nlmax * n * 4));
+  CKR(f->secE.ensure((size_t)2 * g2.H * g2.L * nlmax * n * 4));
+  CKR(f->chain_out.ensure((size_t)cmax * g2.H * CTXT_PARTS * 2 * 2 * n * 4));
   CK(cudaStreamWaitEvent(st, s.prim_done, 0));
   CK(cudaEventRecord(t[4], st));
   const uint32_t l_in = f->S * SIMD;
   const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
-  launch_encode_cols(s.sec_in.as<uint16_t>(), f->ws.A.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
-  launch_encode_rows(f->ws.A.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
-  launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, nl, 1, maps, f->ctx->T, st);
-  launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>(), QV_WORDS_PER_QUERY * n, nb,
-                         f->chain_out.as<uint32_t>(), g2, chain_consts(f->ctx, g2.log2n, 1), f->ctx->T, st);
-  launch_reply(f->chain_out.as<uint32_t>(), nb, g2.H, reply_dev, reply_stride, reply_zq, g2.log2n, f->ctx->T, st);
+  const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
+  for (int c0 = 0; c0 < nb; c0 += SEC_CHUNK) {
+    const int nc = std::min(SEC_CHUNK, nb - c0);
+    const int nl = CTXT_PARTS * nc;
+    const uint16_t* in = s.sec_in.as<uint16_t>() + (size_t)c0 * CTXT_PARTS * l_in * n;
+    launch_encode_cols(in, f->ws.A.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
+    launch_encode_rows(f->ws.A.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
+    launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, nl, 1, maps, f->ctx->T, st);
+    launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>() + (size_t)c0 * QV_WORDS_PER_QUERY * n,
+                           QV_WORDS_PER_QUERY * n, nc, f->chain_out.as<uint32_t>(), g2, cc, f->ctx->T, st);
+    launch_reply(f->chain_out.as<uint32_t>(), nc, g2.H, reply_dev ? reply_dev + (size_t)c0 * reply_stride : nullptr,
+                 reply_stride, reply_zq ? reply_zq + (size_t)c0 * CTXT_PARTS * 2 * n : nullptr, g2.log2n, f->ctx->T,
+                 st);
+  }
   if (host_reply)
     CK(cudaMemcpyAsync(host_reply, reply_dev, (size_t)nb * dnspir_reply_bytes(), cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(t[5], st));
@@ -165,6 +214,14 @@ int fleet_drain(dnspir_fleet* f) {
   CK(cudaStreamSynchronize(f->st));
   CK(cudaStreamSynchronize(f->sec));
   for (auto& s : f->slot) s.sec_pending = false;
+  if (f->engine == DNSPIR_ENGINE_TENSOR) {
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, f->err_word.p, 4, cudaMemcpyDeviceToHost));
+    if (e) {
+      CK(cudaMemset(f->err_word.p, 0, 4));
+      return fail(DNSPIR_ERR_TIMEOUT, "tensor scan: a pipeline wait gave up");
+    }
+  }
   return DNSPIR_OK;
 }
 
@@ -238,7 +295,6 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   }
   CKR(f->slabs_dev.ensure(num_shards * sizeof(uint32_t*)));
   CKR(f->distinct_dev.ensure(num_shards * sizeof(int)));
-  CKR(f->counter.ensure(sizeof(uint32_t)));
   CK(cudaMemcpy(f->slabs_dev.p, ptrs.data(), num_shards * sizeof(uint32_t*), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(f->distinct_dev.p, dist.data(), num_shards * sizeof(int), cudaMemcpyHostToDevice));
   CKR(f->a_zq.ensure((size_t)num_distinct * SIMD * f->g1.n * 8));
@@ -255,10 +311,151 @@ int dnspir_fleet_create(int device, uint64_t num_entries, uint32_t num_distinct,
 
 int dnspir_fleet_set_batch(dnspir_fleet* f, uint32_t max_batch) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
-  if (!scan_batch_supported((int)max_batch)) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1, 2, 4, 8 or 16");
   std::lock_guard<std::mutex> lk(f->mu);
+  if (f->engine == DNSPIR_ENGINE_TENSOR) {
+    if (max_batch < 1 || max_batch > TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
+  } else if (!scan_batch_supported((int)max_batch)) {
+    return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1, 2, 4, 8 or 16");
+  }
   f->batch = (int)max_batch;
   return DNSPIR_OK;
+}
+
+int dnspir_fleet_set_engine(dnspir_fleet* f, int engine) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  if (engine != DNSPIR_ENGINE_CUDA_CORES && engine != DNSPIR_ENGINE_TENSOR)
+    return fail(DNSPIR_ERR_BAD_ARG, "unknown scan engine");
+  if (engine == DNSPIR_ENGINE_TENSOR && !tensor_layout_supported(f->g1))
+    return fail(DNSPIR_ERR_BAD_SHAPE, "the tensor layout needs loop_len = N/2 and N >= 256");
+  DeviceGuard dg(f->device);
+  if (engine == DNSPIR_ENGINE_TENSOR) {
+    CKR(f->err_word.ensure(4));
+    CK(cudaMemset(f->err_word.p, 0, 4));
+  }
+  if (engine != f->engine)
+    for (uint32_t d = 0; d < f->D; d++) f->ready[d] = false;  // the slab layout changes
+  f->engine = engine;
+  f->batch = 1;
+  f->tuned.clear();
+  return DNSPIR_OK;
+}
+
+int dnspir_fleet_tune(dnspir_fleet* f, uint32_t batch, double* ms_per_shape, int* chosen) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  if (f->engine != DNSPIR_ENGINE_TENSOR) return fail(DNSPIR_ERR_BAD_ARG, "tuning applies to the tensor engine");
+  if (batch < 1 || batch > (uint32_t)TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
+  CKR(fleet_ready(f));
+  DeviceGuard dg(f->device);
+  const Group& g1 = f->g1;
+  const size_t n = g1.n;
+  int count = 0;
+  const TScanShape* sh = tscan_shapes(&count);
+  const int nb = (int)batch;
+  int max_pad = nb;
+  for (int i = 0; i < count; i++) {
+    const int q = sh[i].nq / 4;
+    max_pad = std::max(max_pad, (nb + q - 1) / q * q);
+  }
+  // zero queries: the scan's time does not depend on the values
+  DBuf qnat, out, qb;
+  CKR(qnat.ensure((size_t)max_pad * QV_WORDS_PER_QUERY * n * 4));
+  CKR(out.ensure((size_t)nb * f->S * 2 * n * SIMD * 4));
+  CKR(qb.ensure(tscan_query_bytes(g1, max_pad)));
+  CK(cudaMemsetAsync(qnat.p, 0, (size_t)max_pad * QV_WORDS_PER_QUERY * n * 4, f->st));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e30;
+  int best_i = -1;
+  for (int i = 0; i < count; i++) {
+    const int q = sh[i].nq / 4;
+    const int pad = (nb + q - 1) / q * q;
+    double ms = -1;
+    // the shape is a candidate when the padding costs at most a factor 2
+    if (pad <= 2 * nb || q <= 4) {
+      bool ok = true;
+      float t = 0, tot = 0;
+      for (int r = 0; r < 3 && ok; r++) {
+        cudaEventRecord(e0, f->st);
+        ok = launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, nb, pad,
+                          qb.as<uint8_t>(), out.as<uint32_t>(), f->err_word.as<uint32_t>(), g1,
+                          slot_maps(f->ctx, g1.log2n), sh[i], f->st) == 0;
+        cudaEventRecord(e1, f->st);
+        if (ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) {
+          if (r > 0) tot += t;  // the first run warms up
+        } else {
+          ok = false;
+        }
+      }
+      cudaGetLastError();
+      if (ok) ms = tot / 2;
+    }
+    if (ms_per_shape) ms_per_shape[i] = ms;
+    if (ms > 0 && ms < best) {
+      best = ms;
+      best_i = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaStreamSynchronize(f->st));
+  uint32_t e = 0;
+  CK(cudaMemcpy(&e, f->err_word.p, 4, cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(f->err_word.p, 0, 4));
+    return fail(DNSPIR_ERR_TIMEOUT, "tensor scan: a pipeline wait gave up");
+  }
+  if (best_i < 0) return fail(DNSPIR_ERR_CUDA, "no tile shape ran");
+  f->tuned[nb] = best_i;
+  if (chosen) *chosen = best_i;
+  return DNSPIR_OK;
+}
+
+int dnspir_fleet_scan(dnspir_fleet* f, const uint32_t* qnat_dev, uint32_t nq, uint32_t* out_dev) {
+  if (!f || (nq && (!qnat_dev || !out_dev))) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(f->mu);
+  CKR(fleet_ready(f));
+  DeviceGuard dg(f->device);
+  const Group& g1 = f->g1;
+  const size_t n = g1.n, qv = QV_WORDS_PER_QUERY * n;
+  const size_t per_out = (size_t)f->S * 2 * n * SIMD;
+  QSlot& s = f->slot[0];
+  CKR(slot_acquire(f, s));
+  for (uint32_t g0 = 0; g0 < nq; g0 += f->batch) {
+    const int nb = (int)std::min<uint32_t>(f->batch, nq - g0);
+    int Bk = kernel_batch(nb);
+    if (f->engine == DNSPIR_ENGINE_TENSOR) tensor_shape(f, nb, &Bk);
+    CKR(slot_workspace(f, s, Bk, nb));
+    CK(cudaMemcpyAsync(s.qnat.p, qnat_dev + g0 * qv, (size_t)nb * qv * 4, cudaMemcpyDeviceToDevice, f->st));
+    if (Bk > nb) CK(cudaMemsetAsync(s.qnat.as<uint32_t>() + nb * qv, 0, (size_t)(Bk - nb) * qv * 4, f->st));
+    if (f->engine == DNSPIR_ENGINE_TENSOR) {
+      int pad = 0;
+      const TScanShape& shape = tensor_shape(f, nb, &pad);
+      if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), qv, nb, Bk, f->qb.as<uint8_t>(),
+                       s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), shape,
+                       f->st))
+        return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
+    } else if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), qv, Bk,
+                                 s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), f->st)) {
+      return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
+    }
+    CK(cudaMemcpyAsync(out_dev + g0 * per_out, s.fin.p, (size_t)nb * per_out * 4, cudaMemcpyDeviceToDevice, f->st));
+  }
+  CK(cudaGetLastError());
+  return fleet_drain(f);
+}
+
+int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int max) {
+  int count = 0;
+  const TScanShape* sh = tscan_shapes(&count);
+  for (int i = 0; i < count && i < max; i++) {
+    if (nq) nq[i] = sh[i].nq;
+    if (mtpc) mtpc[i] = sh[i].mtpc;
+    if (stages) stages[i] = sh[i].stages;
+  }
+  return count;
 }
 
 int dnspir_fleet_set_shards(dnspir_fleet* f, uint32_t first, uint32_t count, const uint16_t* entries,
@@ -278,9 +475,28 @@ int dnspir_fleet_set_shards(dnspir_fleet* f, uint32_t first, uint32_t count, con
       src = f->ws.in16.as<uint16_t>();
     }
     for (uint32_t i = 0; i < cnt; i++) f->ready[first + b0 + i] = false;
-    CKR(preprocess_shards(f->ctx, f->g1, 0, &f->slabs[first + b0], (int)cnt, src,
-                          f->a_zq.as<uint64_t>() + (size_t)(first + b0) * SIMD * f->g1.n,
-                          f->a_ms.as<uint32_t>() + (size_t)(first + b0) * SIMD * f->g1.n, f->ws, f->st));
+    if (f->engine == DNSPIR_ENGINE_TENSOR) {
+      // preprocess into lane-layout scratch, then re-tile into the fleet slab
+      const uint32_t tb = 4;
+      const size_t words = slab_words(f->g1);
+      CKR(f->tmp_lane.ensure((size_t)std::min(cnt, tb) * words * 4));
+      for (uint32_t c0 = 0; c0 < cnt; c0 += tb) {
+        const uint32_t cc = std::min(tb, cnt - c0);
+        std::vector<uint32_t*> tmp(cc);
+        for (uint32_t i = 0; i < cc; i++) tmp[i] = f->tmp_lane.as<uint32_t>() + i * words;
+        CKR(preprocess_shards(f->ctx, f->g1, 0, tmp.data(), (int)cc, src + (size_t)c0 * per,
+                              f->a_zq.as<uint64_t>() + (size_t)(first + b0 + c0) * SIMD * f->g1.n,
+                              f->a_ms.as<uint32_t>() + (size_t)(first + b0 + c0) * SIMD * f->g1.n, f->ws, f->st));
+        for (uint32_t i = 0; i < cc; i++)
+          launch_retile(tmp[i], reinterpret_cast<uint8_t*>(f->slabs[first + b0 + c0 + i]), f->g1, f->st);
+      }
+      CK(cudaStreamSynchronize(f->st));
+      f->tmp_lane.release();
+    } else {
+      CKR(preprocess_shards(f->ctx, f->g1, 0, &f->slabs[first + b0], (int)cnt, src,
+                            f->a_zq.as<uint64_t>() + (size_t)(first + b0) * SIMD * f->g1.n,
+                            f->a_ms.as<uint32_t>() + (size_t)(first + b0) * SIMD * f->g1.n, f->ws, f->st));
+    }
     for (uint32_t i = 0; i < cnt; i++) f->ready[first + b0 + i] = true;
   }
   return DNSPIR_OK;
@@ -321,7 +537,8 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
   uint32_t gi = 0;
   for (size_t g0 = 0; g0 < ok.size(); g0 += f->batch, gi++) {
     const int nb = (int)std::min<size_t>(f->batch, ok.size() - g0);
-    const int Bk = kernel_batch(nb);
+    int Bk = kernel_batch(nb);
+    if (f->engine == DNSPIR_ENGINE_TENSOR) tensor_shape(f, nb, &Bk);
     QSlot& s = f->slot[gi & 1];
     cudaEvent_t* t = nullptr;
     CKR(group_events(f, gi, &t));

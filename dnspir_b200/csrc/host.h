@@ -60,6 +60,11 @@ struct DBuf {
   T* as() const {
     return (T*)p;
   }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
 };
 
 // RAII pinned host buffer (asynchronous copies need page-locked memory)

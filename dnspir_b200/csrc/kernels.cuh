@@ -79,10 +79,31 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
 // ---- primary scan (main_pir_loop, base_pir.rs:1085-1247)
 // B queries (B in {1, 2, 4, 8, 16}) per pass over all shards.  qnat: per query
 // [slot][p][N] natural order (slots 0 gk0, 1 gk1, 2 pq, 3 pqc), q_stride words
-// apart.  out: [b][s][p][u][lane] reduced mod p.  counter: one device word.
+// apart.  out: [b][s][p][u][lane] reduced mod p.
 int scan_batch_supported(int B);
 int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int B,
-                      uint32_t* out, const Group& g, const SlotMaps& maps, uint32_t* counter, cudaStream_t st);
+                      uint32_t* out, const Group& g, const SlotMaps& maps, cudaStream_t st);
+// ---- primary scan on the tensor cores (tscan.cu): 8-bit limbs, kind::i8
+// Tensor layout: the slab indexed by query slot, bytes in 128 x 128 blocks
+// [p][sign][m-tile][k-chunk] (same size as the lane layout).  Needs loop_len
+// = N/2 and N >= 256.
+struct TScanShape {
+  int nq;      // rows of the query operand per CTA (4 limbs x queries)
+  int mtpc;    // 128-row m-tiles per CTA
+  int stages;  // shared-memory pipeline depth
+};
+int tensor_layout_supported(const Group& g);
+void tensor_dims(const Group& g, uint32_t* mt_total, uint32_t* kc_total);
+void launch_retile(const uint32_t* lane_slab, uint8_t* tensor_slab, const Group& g, cudaStream_t st);
+const TScanShape* tscan_shapes(int* count);
+size_t tscan_query_bytes(const Group& g, int nb_pad);
+// nb queries (decoded, qnat) padded to nb_pad (a multiple of shape.nq / 4);
+// qb: tscan_query_bytes of workspace; out as launch_scan_batch; err: one
+// device word set to 1 when a bounded wait gave up.  Returns -1 for a shape
+// that does not fit.
+int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int nb, int nb_pad,
+                 uint8_t* qb, uint32_t* out, uint32_t* err, const Group& g, const SlotMaps& maps,
+                 const TScanShape& shape, cudaStream_t st);
 // Per-lane queries (perform_pir_split): qlane [(lane*4 + v)*2 + p][N] natural order;
 // part: [chunk][p][u][lane], chunks = H * R.
 int scan_chunks(const Group& g, int nshards);
@@ -90,9 +111,10 @@ void launch_scan_lanes(const uint32_t* slab, const uint32_t* qlane, uint32_t* pa
                        const SlotMaps& maps, cudaStream_t st);
 // Primary epilogue for nq queries: scan output -> b (iNTT, CRT), mod-switch,
 // combine with the shard's a-part, three base-1025 digits -> secondary
-// entries sec_in[t = s*8+lane][q*3 + part][n].
+// entries.  Queries are grouped in chunks of `chunk`; chunk c starts at
+// c * chunk * 3 * nshards * 8 * N and holds [t = s*8+lane][q*3 + part][n].
 void launch_primary_epilogue(const uint32_t* fin, int nq, int nshards, const uint32_t* a_ms, const int* distinct_of,
-                             uint16_t* sec_in, const Group& g, const SlotMaps& maps, const NttTables& T,
+                             uint16_t* sec_in, int chunk, const Group& g, const SlotMaps& maps, const NttTables& T,
                              cudaStream_t st);
 // Epilogue returning b as Z_q coefficients [lane][n] (shard-level perform_pir_split).
 void launch_epilogue_zq(const uint32_t* part, int chunks, uint64_t* out, const Group& g, const SlotMaps& maps,

@@ -14,7 +14,9 @@
 // its rows contiguously.  Products of canonical residues are below 2^52, so one
 // 64-bit accumulator per (lane, query) absorbs a half (3 * L <= 3072 products)
 // without reduction; it is reduced once between halves and once at the end.
-// Blocks take (shard, factor, sign, tile) work items from an atomic counter.
+// One block per (shard, factor, sign, tile) item, consecutive blocks sharing a
+// shard; blocks retire after their item so that the higher-priority secondary
+// stream can take SMs while a scan is running.
 #include "kernels.cuh"
 
 namespace dnspir {
@@ -30,7 +32,6 @@ struct ScanArgs {
   size_t q_stride;       // words between queries
   const uint32_t* gtab;  // (sign, e) position -> odd residue
   uint32_t* out;         // [b][s][p][u][lane], reduced mod p
-  uint32_t* counter;     // work-queue ticket, zeroed before the launch
   int rows;              // rows per window chunk
 };
 
@@ -52,92 +53,81 @@ template <int B, int LPT>
 __global__ void __launch_bounds__(SCAN_NT) scan_batch_kernel(ScanArgs a) {
   constexpr int LG = SIMD / LPT;     // lane groups per slot
   constexpr int TS = SCAN_NT / LG;   // slots per tile
-  extern __shared__ uint32_t win[];  // [3][W][B]
-  __shared__ uint32_t item_s;
+  extern __shared__ uint32_t win[];  // [3][B][W]: x fastest, so a warp's slots hit distinct banks
   const Group& g = a.g;
   const uint32_t N = g.n, half = N / 2, L = g.L;
   const uint32_t R = (uint32_t)a.rows;
   const uint32_t W = TS + R - 1;
   const uint32_t tiles = (half + TS - 1) / TS;
-  const uint32_t items = (uint32_t)a.nshards * 2 * 2 * tiles;
   const int slot = threadIdx.x / LG, lg = threadIdx.x % LG;
   const size_t arr = (size_t)N * SIMD, row_stride = 3 * arr;
-  for (;;) {
-    if (threadIdx.x == 0) item_s = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    const uint32_t item = item_s;
-    __syncthreads();
-    if (item >= items) break;
-    // item = ((s * 2 + p) * 2 + sgn) * tiles + tile: consecutive items share a shard
-    const uint32_t tile = item % tiles;
-    const uint32_t sgn = (item / tiles) & 1;
-    const int p = (item / (2 * tiles)) & 1;
-    const int s = item / (4 * tiles);
-    const uint32_t e0 = tile * TS;
-    const uint32_t e = e0 + slot;
-    const bool active = e < half;
-    const uint32_t u = sgn * half + e;
-    const uint32_t pr = prime_of(p);
-    const uint64_t mu = barrett_mu(pr);
-    const uint32_t* slab = a.slabs[s];
-    uint64_t acc[LPT][B];
+  // item = ((s * 2 + p) * 2 + sgn) * tiles + tile
+  const uint32_t item = blockIdx.x;
+  const uint32_t tile = item % tiles;
+  const uint32_t sgn = (item / tiles) & 1;
+  const int p = (item / (2 * tiles)) & 1;
+  const int s = item / (4 * tiles);
+  const uint32_t e0 = tile * TS;
+  const uint32_t e = e0 + slot;
+  const bool active = e < half;
+  const uint32_t u = sgn * half + e;
+  const uint32_t pr = prime_of(p);
+  const uint64_t mu = barrett_mu(pr);
+  const uint32_t* slab = a.slabs[s];
+  uint64_t acc[LPT][B];
 #pragma unroll
-    for (int l = 0; l < LPT; l++)
+  for (int l = 0; l < LPT; l++)
 #pragma unroll
-      for (int b = 0; b < B; b++) acc[l][b] = 0;
-    for (uint32_t h = 0; h < g.H; h++) {
-      // decoded slots: 0 gk0, 1 gk1, 2 pq, 3 pqc -> window vectors (query of this half, gk0, gk1)
-      const int vslot[3] = {2 + (int)h, 0, 1};
-      for (uint32_t i0 = 0; i0 < L; i0 += R) {
-        const uint32_t i1 = min(L, i0 + R);
-        const uint32_t Wr = TS + (i1 - i0) - 1;
-        const uint32_t w0 = (e0 + L - i1) % half;
-        for (uint32_t idx = threadIdx.x; idx < 3 * Wr * B; idx += SCAN_NT) {
-          const uint32_t b = idx % B, x = (idx / B) % Wr, v = idx / (B * Wr);
-          const uint32_t uu = sgn * half + (w0 + x) % half;
-          const uint32_t kk = (__ldg(a.gtab + uu) - 1) >> 1;
-          win[(v * W + x) * B + b] = __ldg(a.qnat + b * a.q_stride + ((size_t)vslot[v] * 2 + p) * N + kk);
-        }
-        __syncthreads();
-        if (active) {
-          const uint32_t* row = slab + slab_off(g, p, h, i0, 0, u) + lg * LPT;
-          uint32_t x = slot + (i1 - 1 - i0);
+    for (int b = 0; b < B; b++) acc[l][b] = 0;
+  for (uint32_t h = 0; h < g.H; h++) {
+    // decoded slots: 0 gk0, 1 gk1, 2 pq, 3 pqc -> window vectors (query of this half, gk0, gk1)
+    const int vslot[3] = {2 + (int)h, 0, 1};
+    for (uint32_t i0 = 0; i0 < L; i0 += R) {
+      const uint32_t i1 = min(L, i0 + R);
+      const uint32_t Wr = TS + (i1 - i0) - 1;
+      const uint32_t w0 = (e0 + L - i1) % half;
+      for (uint32_t idx = threadIdx.x; idx < 3 * Wr * B; idx += SCAN_NT) {
+        const uint32_t x = idx % Wr, b = (idx / Wr) % B, v = idx / (B * Wr);
+        const uint32_t uu = sgn * half + (w0 + x) % half;
+        const uint32_t kk = (__ldg(a.gtab + uu) - 1) >> 1;
+        win[(v * B + b) * W + x] = __ldg(a.qnat + b * a.q_stride + ((size_t)vslot[v] * 2 + p) * N + kk);
+      }
+      __syncthreads();
+      if (active) {
+        const uint32_t* row = slab + slab_off(g, p, h, i0, 0, u) + lg * LPT;
+        uint32_t x = slot + (i1 - 1 - i0);
 #pragma unroll 2
-          for (uint32_t i = i0; i < i1; i++) {
-            uint32_t ev[LPT], av[LPT], bv[LPT];
-            ld_lanes(row, ev, LPT);
-            ld_lanes(row + arr, av, LPT);
-            ld_lanes(row + 2 * arr, bv, LPT);
-            const uint32_t* wq = win + x * B;
-            const uint32_t* wg0 = win + (W + x) * B;
-            const uint32_t* wg1 = win + (2 * W + x) * B;
+        for (uint32_t i = i0; i < i1; i++) {
+          uint32_t ev[LPT], av[LPT], bv[LPT];
+          ld_lanes(row, ev, LPT);
+          ld_lanes(row + arr, av, LPT);
+          ld_lanes(row + 2 * arr, bv, LPT);
 #pragma unroll
-            for (int b = 0; b < B; b++) {
-              const uint32_t q = wq[b], g0 = wg0[b], g1 = wg1[b];
+          for (int b = 0; b < B; b++) {
+            const uint32_t q = win[b * W + x], g0 = win[(B + b) * W + x], g1 = win[(2 * B + b) * W + x];
 #pragma unroll
-              for (int l = 0; l < LPT; l++)
-                acc[l][b] += (uint64_t)ev[l] * q + (uint64_t)av[l] * g0 + (uint64_t)bv[l] * g1;
-            }
-            row += row_stride;
-            x--;
+            for (int l = 0; l < LPT; l++)
+              acc[l][b] += (uint64_t)ev[l] * q + (uint64_t)av[l] * g0 + (uint64_t)bv[l] * g1;
           }
+          row += row_stride;
+          x--;
         }
-        __syncthreads();
       }
-      if (h + 1 < g.H) {
-#pragma unroll
-        for (int l = 0; l < LPT; l++)
-#pragma unroll
-          for (int b = 0; b < B; b++) acc[l][b] = reduce64(acc[l][b], pr, mu);
-      }
+      __syncthreads();
     }
-    if (active) {
+    if (h + 1 < g.H) {
 #pragma unroll
-      for (int b = 0; b < B; b++) {
-        uint32_t* o = a.out + ((((size_t)b * a.nshards + s) * 2 + p) * N + u) * SIMD + lg * LPT;
+      for (int l = 0; l < LPT; l++)
 #pragma unroll
-        for (int l = 0; l < LPT; l++) o[l] = reduce64(acc[l][b], pr, mu);
-      }
+        for (int b = 0; b < B; b++) acc[l][b] = reduce64(acc[l][b], pr, mu);
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      uint32_t* o = a.out + ((((size_t)b * a.nshards + s) * 2 + p) * N + u) * SIMD + lg * LPT;
+#pragma unroll
+      for (int l = 0; l < LPT; l++) o[l] = reduce64(acc[l][b], pr, mu);
     }
   }
 }
@@ -183,7 +173,7 @@ __global__ void scan_lanes_kernel(const uint32_t* __restrict__ slab, const uint3
 // three base-1025 digits (encode_ciphertext_plaintext, double_pir.rs:70-81).
 __global__ void primary_epilogue_kernel(const uint32_t* __restrict__ fin, int nshards,
                                         const uint32_t* __restrict__ a_ms, const int* __restrict__ distinct_of,
-                                        uint16_t* __restrict__ sec_in, int sec_lanes, Group g,
+                                        uint16_t* __restrict__ sec_in, int nq, int chunk, Group g,
                                         const uint32_t* __restrict__ uof, NttTables T, CrtConst crtc) {
   extern __shared__ uint32_t sm[];  // [l0 q1, l1 q1, l0 q2, l1 q2]
   const int s = blockIdx.x, l0 = blockIdx.y * 2, b = blockIdx.z;
@@ -208,8 +198,11 @@ __global__ void primary_epilogue_kernel(const uint32_t* __restrict__ fin, int ns
     w /= TPLAIN;
     const uint32_t d1 = w % TPLAIN;
     const uint32_t d2 = w / TPLAIN;
+    // the secondary input of queries [c * chunk, ...) is one [t][lanes_c][N] block
+    const int c = b / chunk, bl = b % chunk;
+    const size_t lanes_c = (size_t)CTXT_PARTS * min(chunk, nq - c * chunk);
     const size_t t = (size_t)s * SIMD + l0 + ll;
-    uint16_t* o = sec_in + (t * sec_lanes + (size_t)b * CTXT_PARTS) * N + n;
+    uint16_t* o = sec_in + (size_t)c * chunk * CTXT_PARTS * nshards * SIMD * N + (t * lanes_c + (size_t)bl * CTXT_PARTS) * N + n;
     o[0] = (uint16_t)d0;
     o[N] = (uint16_t)d1;
     o[2 * N] = (uint16_t)d2;
@@ -244,16 +237,9 @@ void launch_batch(const ScanArgs& a, cudaStream_t st) {
   constexpr int TS = SCAN_NT / (SIMD / LPT);
   const size_t smem = (size_t)3 * (TS + a.rows - 1) * B * 4;
   set_smem(scan_batch_kernel<B, LPT>, smem);
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_batch_kernel<B, LPT>, SCAN_NT, smem);
-  if (per_sm < 1) per_sm = 1;
   const uint32_t tiles = (a.g.n / 2 + TS - 1) / TS;
   const uint32_t items = (uint32_t)a.nshards * 4 * tiles;
-  uint32_t grid = (uint32_t)(sms * per_sm);
-  if (grid > items) grid = items;
-  scan_batch_kernel<B, LPT><<<grid, SCAN_NT, smem, st>>>(a);
+  scan_batch_kernel<B, LPT><<<items, SCAN_NT, smem, st>>>(a);
 }
 
 }  // namespace
@@ -270,7 +256,7 @@ static uint32_t inv5_of(uint32_t two_n) {
 int scan_batch_supported(int B) { return B == 1 || B == 2 || B == 4 || B == 8 || B == 16; }
 
 int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int B,
-                      uint32_t* out, const Group& g, const SlotMaps& maps, uint32_t* counter, cudaStream_t st) {
+                      uint32_t* out, const Group& g, const SlotMaps& maps, cudaStream_t st) {
   ScanArgs a;
   a.g = g;
   a.slabs = slabs_dev;
@@ -279,9 +265,7 @@ int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* q
   a.q_stride = q_stride;
   a.gtab = maps.g;
   a.out = out;
-  a.counter = counter;
   a.rows = (int)(g.L < 256 ? g.L : 256);
-  if (cudaMemsetAsync(counter, 0, sizeof(uint32_t), st) != cudaSuccess) return -1;
   switch (B) {
     case 1: launch_batch<1, 8>(a, st); break;
     case 2: launch_batch<2, 8>(a, st); break;
@@ -313,12 +297,12 @@ void launch_scan_lanes(const uint32_t* slab, const uint32_t* qlane, uint32_t* pa
 }
 
 void launch_primary_epilogue(const uint32_t* fin, int nq, int nshards, const uint32_t* a_ms, const int* distinct_of,
-                             uint16_t* sec_in, const Group& g, const SlotMaps& maps, const NttTables& T,
+                             uint16_t* sec_in, int chunk, const Group& g, const SlotMaps& maps, const NttTables& T,
                              cudaStream_t st) {
   const size_t smem = (size_t)4 * g.n * 4;
   dim3 grid(nshards, SIMD / 2, nq);
   set_smem(primary_epilogue_kernel, smem);
-  primary_epilogue_kernel<<<grid, 256, smem, st>>>(fin, nshards, a_ms, distinct_of, sec_in, CTXT_PARTS * nq, g,
+  primary_epilogue_kernel<<<grid, 256, smem, st>>>(fin, nshards, a_ms, distinct_of, sec_in, nq, chunk, g,
                                                    maps.uof, T, host_crt_const());
 }
 

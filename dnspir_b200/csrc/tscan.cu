@@ -1,0 +1,458 @@
+// tscan.cu -- the primary scan (main_pir_loop, crates/pir/src/base_pir.rs:
+// 1085-1247) for a batch of queries on the tensor cores, exact over 8-bit limbs.
+//
+// With loop_len L = N/2 (every primary group at N = 2048, IndexGroup,
+// base_pir.rs:168-174) each output slot u = (sign, e) meets every query slot
+// d = (e + L - 1 - i) mod L of its sign exactly once, at row i.  Indexing the
+// slab by d instead of i turns the scan, per (shard, factor p, sign), into a
+// product of integer matrices
+//     out[(e, lane), b] = sum_{K = (h, a, d)} A[(e, lane), K] * V[K, b]
+// with A the slab (E, G0, G1 of each half h) and V the B queries (the query of
+// half h, gk0, gk1 at slot (sign, d)).  Both factors are below 2^32 and split
+// into four 8-bit limbs (the bytes of the word): tcgen05.mma kind::i8 forms the
+// 16 limb products with u8 x u8 -> s32 accumulation, at most
+// K * 255^2 <= 6144 * 65025 < 2^31 per entry, so no partial sum overflows;
+// the epilogue recombines sum_{k,j} D_kj * (2^(8(k+j)) mod p) < 2^59 in 64 bits
+// and reduces it mod p.  The result is the same residue as the CUDA-core scan.
+//
+// Tensor layout of one shard (bytes), blocks [p][sign][mt][kc] of 16 KiB: each
+// block is 128 rows x 128 bytes in the 128-byte-swizzled K-major form the MMA
+// reads (16-byte unit c of row r stored at unit c ^ (r mod 8)).  Row r of
+// m-tile mt is limb r mod 4 of lane (r / 4) mod 8 of slot e = 4 mt + r / 32;
+// byte kb of K-chunk kc is K index kk = 128 kc + kb = (h * 3 + a) * L + d.
+// The query operand has the same form: [p][sign][kc][n = 4 b + j][128 bytes].
+//
+// One CTA of 128 threads per (shard, p, sign, m-tiles, query group): thread 0
+// streams A and V chunks into a ring of shared-memory stages with bulk copies,
+// thread 32 issues the MMAs into a TMEM accumulator, then all four warps read
+// their 32 TMEM lanes and write the reduced residues.  Every wait is bounded;
+// a wait that gives up sets an error word, and the CTA still waits for its
+// copies in flight and frees its TMEM before returning.
+#include "kernels.cuh"
+
+namespace dnspir {
+namespace {
+
+constexpr uint32_t TBLK = 16384;  // one 128 x 128-byte block
+constexpr int TSCAN_NT = 128;
+constexpr uint64_t WAIT_NS = 2000000000ull;
+
+__device__ __forceinline__ uint32_t sa(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(sa(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the phase of `parity` to complete; false after WAIT_NS.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = gtimer();
+  while (!mbar_try(bar, parity))
+    if (gtimer() - t0 > WAIT_NS) return false;
+  return true;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   sa(dst)),
+               "l"(src), "r"(bytes), "r"(sa(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzle, 8-row groups 1024 bytes apart (tcgen05 shared
+// memory descriptor: start >> 4, LBO >> 4, SBO >> 4, version 1, layout 2).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor, kind::i8: D s32, A and B unsigned 8-bit, both K-major.
+__host__ __device__ constexpr uint32_t idesc_u8(int M, int N) {
+  return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_u8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sa(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct TScanArgs {
+  const uint8_t* const* slabs;  // per shard, tensor layout
+  int nshards;
+  const uint8_t* qb;  // query operand [p][sign][kc][nq_rows][128]
+  uint32_t nq_rows;   // rows of the query operand: 4 x padded batch
+  uint32_t nvalid;    // queries whose results are written
+  uint32_t* out;      // [b][s][p][u][lane]
+  uint32_t* err;      // set to 1 when a wait gives up
+  uint32_t half, mt_total, kc_total, groups, stages;
+};
+
+template <int NQ, int MTPC>
+__global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
+  constexpr uint32_t A_BYTES = MTPC * TBLK;
+  constexpr uint32_t STAGE = A_BYTES + NQ * 128;
+  constexpr uint32_t COLS = (MTPC * NQ) <= 32 ? 32 : (MTPC * NQ);
+  constexpr int NSPLIT = NQ > 256 ? NQ / 256 : 1;
+  constexpr int NMMA = NQ / NSPLIT;
+  static_assert(STAGE % 1024 == 0 && COLS <= 512 && (COLS & (COLS - 1)) == 0, "tile shape");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t S_ = a.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + S_ * STAGE);
+  uint64_t* empty = full + S_;
+  uint64_t* accb = empty + S_;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(accb + 1);
+  volatile uint32_t* issued_s = tslot + 1;
+  volatile uint32_t* consumed_s = tslot + 2;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+
+  // item = (((s * 2 + p) * 2 + sign) * mtc + mtc_i) * groups + grp
+  uint32_t item = blockIdx.x;
+  const uint32_t grp = item % a.groups;
+  item /= a.groups;
+  const uint32_t mtc = a.mt_total / MTPC;
+  const uint32_t mt0 = (item % mtc) * MTPC;
+  item /= mtc;
+  const uint32_t sgn = item & 1;
+  const int p = (item >> 1) & 1;
+  const int s = item >> 2;
+  const uint32_t KC = a.kc_total;
+  const size_t ps = (size_t)p * 2 + sgn;
+  const uint8_t* abase = a.slabs[s] + (ps * a.mt_total + mt0) * KC * TBLK;
+  const uint8_t* bbase = a.qb + ps * KC * a.nq_rows * 128 + (size_t)grp * NQ * 128;
+
+  if (threadIdx.x == 0) {
+    for (uint32_t i = 0; i < S_; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(accb, 1);
+    *issued_s = 0;
+    *consumed_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(tslot)), "r"(COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  if (threadIdx.x == 0) {
+    // producer: chunk kc of every m-tile and of the query group into stage kc % S_
+    uint32_t issued = 0;
+    for (uint32_t kc = 0; kc < KC; kc++) {
+      const uint32_t st = kc % S_, n = kc / S_;
+      if (n > 0 && !mbar_wait(&empty[st], (n - 1) & 1)) {
+        atomicOr(a.err, 1u);
+        break;
+      }
+      uint8_t* dst = sm + st * STAGE;
+      mbar_expect_tx(&full[st], STAGE);
+#pragma unroll
+      for (int t = 0; t < MTPC; t++) bulk_g2s(dst + t * TBLK, abase + ((size_t)t * KC + kc) * TBLK, TBLK, &full[st]);
+      bulk_g2s(dst + A_BYTES, bbase + (size_t)kc * a.nq_rows * 128, NQ * 128, &full[st]);
+      issued = kc + 1;
+    }
+    *issued_s = issued;
+  } else if (threadIdx.x == 32) {
+    // MMA issuer
+    constexpr uint32_t idesc = idesc_u8(128, NMMA);
+    uint32_t consumed = 0;
+    for (uint32_t kc = 0; kc < KC; kc++) {
+      const uint32_t st = kc % S_, n = kc / S_;
+      if (!mbar_wait(&full[st], n & 1)) {
+        atomicOr(a.err, 1u);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t s0 = sa(sm + st * STAGE);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+#pragma unroll
+        for (int t = 0; t < MTPC; t++) {
+#pragma unroll
+          for (int ns = 0; ns < NSPLIT; ns++)
+            mma_u8(tmem + t * NQ + ns * NMMA, sw128_desc(s0 + t * TBLK + 32 * k),
+                   sw128_desc(s0 + A_BYTES + ns * NMMA * 128 + 32 * k), idesc, (kc | k) != 0);
+        }
+      }
+      mma_commit(&empty[st]);
+      consumed = kc + 1;
+    }
+    *consumed_s = consumed;
+    mma_commit(accb);
+  }
+  __syncwarp();
+
+  // epilogue: warp w holds TMEM lanes 32w..32w+31 = rows of slot e = 4 mt + w
+  const bool acc_ok = mbar_wait(accb, 0);
+  tc_fence_after();
+  if (acc_ok) {
+    const uint32_t pr = prime_of(p);
+    const uint64_t mu = barrett_mu(pr);
+    uint64_t cw[7];
+    cw[0] = 1;
+    cw[1] = 256;
+    cw[2] = 65536;
+    cw[3] = reduce64(1ull << 24, pr, mu);
+    cw[4] = reduce64(1ull << 32, pr, mu);
+    cw[5] = reduce64(cw[4] << 8, pr, mu);
+    cw[6] = reduce64(cw[5] << 8, pr, mu);
+    const int k = lane & 3, l8 = lane >> 2;
+    const uint64_t c0 = k == 0 ? cw[0] : k == 1 ? cw[1] : k == 2 ? cw[2] : cw[3];
+    const uint64_t c1 = k == 0 ? cw[1] : k == 1 ? cw[2] : k == 2 ? cw[3] : cw[4];
+    const uint64_t c2 = k == 0 ? cw[2] : k == 1 ? cw[3] : k == 2 ? cw[4] : cw[5];
+    const uint64_t c3 = k == 0 ? cw[3] : k == 1 ? cw[4] : k == 2 ? cw[5] : cw[6];
+    const uint32_t N = 2 * a.half;
+    for (int t = 0; t < MTPC; t++) {
+      const uint32_t u = sgn * a.half + 4 * (mt0 + t) + warp;
+#pragma unroll 1
+      for (int q4 = 0; q4 < NQ / 16; q4++) {
+        uint32_t v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + t * NQ + 16 * q4, v);
+        uint64_t tot[4];
+#pragma unroll
+        for (int qq = 0; qq < 4; qq++) {
+          uint64_t x = (uint64_t)v[4 * qq] * c0 + (uint64_t)v[4 * qq + 1] * c1 + (uint64_t)v[4 * qq + 2] * c2 +
+                       (uint64_t)v[4 * qq + 3] * c3;
+          x += __shfl_xor_sync(0xffffffffu, x, 1);
+          x += __shfl_xor_sync(0xffffffffu, x, 2);
+          tot[qq] = x;
+        }
+        const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
+        const uint32_t bq = grp * (NQ / 4) + 4 * q4 + k;
+        if (bq < a.nvalid)
+          a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicOr(a.err, 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // copies issued but never consumed (only after a wait gave up) must land
+    // before the shared memory is released
+    for (uint32_t kc = *consumed_s; kc < *issued_s; kc++) mbar_wait(&full[kc % S_], (kc / S_) & 1);
+  }
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+  }
+}
+
+// Lane layout (slab_off) -> tensor layout; one thread per 16-byte unit.
+__global__ void retile_kernel(const uint32_t* __restrict__ src, uint8_t* __restrict__ dst, Group g, uint32_t mt_total,
+                              uint32_t kc_total) {
+  const uint32_t half = g.n / 2;
+  const size_t total = (size_t)4 * mt_total * kc_total * 1024;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const uint32_t c = idx & 7, r = (idx >> 3) & 127;
+  size_t blk = idx >> 10;
+  const uint32_t kc = blk % kc_total;
+  blk /= kc_total;
+  const uint32_t mt = blk % mt_total;
+  blk /= mt_total;
+  const uint32_t sgn = blk & 1;
+  const int p = (int)(blk >> 1);
+  const uint32_t e = 4 * mt + r / 32, lane = (r / 4) & 7, limb = r & 3;
+  const uint32_t u = sgn * half + e;
+  const uint32_t kk0 = kc * 128 + c * 16;  // 16 consecutive K indices of one (h, a)
+  const uint32_t ha = kk0 / half, d0 = kk0 % half;
+  const uint32_t h = ha / 3, a = ha % 3;
+  uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int x = 0; x < 16; x++) {
+    const uint32_t d = d0 + x;
+    const uint32_t i = (e + 2 * half - 1 - d) % half;  // row i meets slot d (loop_len = N/2)
+    const uint32_t v = __ldg(src + slab_off(g, p, h, i, a, u) + lane);
+    w[x >> 2] |= ((v >> (8 * limb)) & 0xFFu) << (8 * (x & 3));
+  }
+  uint8_t* o = dst + ((((size_t)p * 2 + sgn) * mt_total + mt) * kc_total + kc) * TBLK + r * 128 + ((c ^ (r & 7)) << 4);
+  *reinterpret_cast<uint4*>(o) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Query operand: one thread per (p, sign, query, 16-byte K unit); writes the
+// four limb rows 4b + j.  Queries b >= nb are zero.
+__global__ void tquery_kernel(const uint32_t* __restrict__ qnat, size_t q_stride, uint32_t nb, uint32_t nb_pad,
+                              uint8_t* __restrict__ qb, Group g, const uint32_t* __restrict__ gtab,
+                              uint32_t kc_total) {
+  const uint32_t half = g.n / 2, N = g.n;
+  const uint32_t units = kc_total * 8;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)4 * nb_pad * units) return;
+  const uint32_t cu = idx % units;
+  const uint32_t b = (idx / units) % nb_pad;
+  const uint32_t ps = (uint32_t)(idx / ((size_t)units * nb_pad));
+  const uint32_t sgn = ps & 1;
+  const int p = (int)(ps >> 1);
+  const uint32_t kk0 = cu * 16;
+  const uint32_t ha = kk0 / half, d0 = kk0 % half;
+  const uint32_t h = ha / 3, a = ha % 3;
+  const uint32_t slot = a == 0 ? 2 + h : a - 1;  // decoded slots: 0 gk0, 1 gk1, 2 pq, 3 pqc
+  uint32_t w[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) w[j][q] = 0;
+  if (b < nb) {
+    const uint32_t* src = qnat + (size_t)b * q_stride + ((size_t)slot * 2 + p) * N;
+#pragma unroll
+    for (int x = 0; x < 16; x++) {
+      const uint32_t k = (__ldg(gtab + sgn * half + d0 + x) - 1) >> 1;
+      const uint32_t v = __ldg(src + k);
+#pragma unroll
+      for (int j = 0; j < 4; j++) w[j][x >> 2] |= ((v >> (8 * j)) & 0xFFu) << (8 * (x & 3));
+    }
+  }
+  const uint32_t kc = cu / 8, c = cu % 8;
+  const uint32_t rows = 4 * nb_pad;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const uint32_t r = 4 * b + j;
+    uint8_t* o = qb + (((size_t)ps * kc_total + kc) * rows + r) * 128 + ((c ^ (r & 7)) << 4);
+    *reinterpret_cast<uint4*>(o) = make_uint4(w[j][0], w[j][1], w[j][2], w[j][3]);
+  }
+}
+
+template <int NQ, int MTPC>
+int launch_t(const TScanArgs& a0, int stages, cudaStream_t st) {
+  TScanArgs a = a0;
+  a.stages = (uint32_t)stages;
+  constexpr uint32_t STAGE = MTPC * TBLK + NQ * 128;
+  const size_t smem = 1024 + (size_t)stages * STAGE + (2 * stages + 1) * 8 + 16;
+  if (smem > 227 * 1024) return -1;
+  set_smem(tscan_kernel<NQ, MTPC>, smem);
+  // resident CTAs must not ask for more TMEM columns than the SM has
+  constexpr int COLS = (MTPC * NQ) <= 32 ? 32 : (MTPC * NQ);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tscan_kernel<NQ, MTPC>, TSCAN_NT, smem);
+  if (per_sm * COLS > 512) return -1;
+  const size_t items = (size_t)a.nshards * 4 * (a.mt_total / MTPC) * a.groups;
+  tscan_kernel<NQ, MTPC><<<(unsigned)items, TSCAN_NT, smem, st>>>(a);
+  return 0;
+}
+
+}  // namespace
+
+int tensor_layout_supported(const Group& g) { return g.log2n >= 8 && g.L == g.n / 2 && g.H >= 1; }
+
+void tensor_dims(const Group& g, uint32_t* mt_total, uint32_t* kc_total) {
+  *mt_total = (g.n / 2) * SIMD * 4 / 128;
+  *kc_total = 3 * g.H * (g.n / 2) / 128;
+}
+
+void launch_retile(const uint32_t* lane_slab, uint8_t* tensor_slab, const Group& g, cudaStream_t st) {
+  uint32_t mt, kc;
+  tensor_dims(g, &mt, &kc);
+  const size_t total = (size_t)4 * mt * kc * 1024;
+  retile_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(lane_slab, tensor_slab, g, mt, kc);
+}
+
+// The tile shapes: queries per CTA (NQ / 4) and m-tiles per CTA.
+const TScanShape* tscan_shapes(int* count) {
+  // stages chosen so that the shapes with 1 m-tile and up to 128 rows fit two
+  // CTAs per SM
+  static const TScanShape shapes[] = {
+      {16, 1, 5},  {16, 1, 10}, {32, 1, 5},  {64, 1, 4},  {64, 2, 3},  {128, 1, 3},
+      {128, 2, 3}, {256, 1, 3}, {256, 1, 4}, {256, 2, 2}, {256, 2, 3},
+  };
+  *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
+  return shapes;
+}
+
+size_t tscan_query_bytes(const Group& g, int nb_pad) {
+  uint32_t mt, kc;
+  tensor_dims(g, &mt, &kc);
+  return (size_t)4 * kc * 4 * nb_pad * 128;
+}
+
+int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int nb, int nb_pad,
+                 uint8_t* qb, uint32_t* out, uint32_t* err, const Group& g, const SlotMaps& maps,
+                 const TScanShape& shape, cudaStream_t st) {
+  uint32_t mt, kc;
+  tensor_dims(g, &mt, &kc);
+  const int qpc = shape.nq / 4;
+  if (nb_pad % qpc || nb_pad < qpc || mt % shape.mtpc) return -1;
+  {
+    const size_t threads = (size_t)4 * nb_pad * kc * 8;
+    tquery_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(qnat, q_stride, nb, nb_pad, qb, g, maps.g, kc);
+  }
+  TScanArgs a;
+  a.slabs = slabs_dev;
+  a.nshards = nshards;
+  a.qb = qb;
+  a.nq_rows = 4 * nb_pad;
+  a.nvalid = nb;
+  a.out = out;
+  a.err = err;
+  a.half = g.n / 2;
+  a.mt_total = mt;
+  a.kc_total = kc;
+  a.groups = nb_pad / qpc;
+  a.stages = 0;
+  const int stg = shape.stages;
+  switch (shape.nq * 10 + shape.mtpc) {
+    case 161: return launch_t<16, 1>(a, stg, st);
+    case 321: return launch_t<32, 1>(a, stg, st);
+    case 641: return launch_t<64, 1>(a, stg, st);
+    case 642: return launch_t<64, 2>(a, stg, st);
+    case 1281: return launch_t<128, 1>(a, stg, st);
+    case 1282: return launch_t<128, 2>(a, stg, st);
+    case 2561: return launch_t<256, 1>(a, stg, st);
+    case 2562: return launch_t<256, 2>(a, stg, st);
+    default: return -1;
+  }
+}
+
+}  // namespace dnspir

@@ -107,10 +107,40 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
  * dns/server.rs:707-728).  entries: count x (8 primary_order N) coefficients. */
 int dnspir_fleet_set_shards(dnspir_fleet* fleet, uint32_t first_distinct, uint32_t count, const uint16_t* entries,
                             int entries_on_device);
-/* Queries answered per pass over the shard slabs (1, 2, 4, 8 or 16; default
- * 1).  dnspir_fleet_process_queries splits its queries into groups of this
- * size; every group reads each slab once.  Replies do not depend on it. */
+/* Queries answered per pass over the shard slabs (default 1): 1, 2, 4, 8 or
+ * 16 on the CUDA-core engine, 1..256 on the tensor engine.
+ * dnspir_fleet_process_queries splits its queries into groups of this size;
+ * every group reads each slab once.  Replies do not depend on it.  The
+ * reference answers one query per pass (process_queries, pir_wrapper.rs:349
+ * takes at most two, one per database); batching has no counterpart there. */
 int dnspir_fleet_set_batch(dnspir_fleet* fleet, uint32_t max_batch);
+
+/* Scan engine of a fleet.  CUDA_CORES (default): the slab in lane layout, 64-bit
+ * multiply-accumulate per 32-bit residue.  TENSOR: the slab re-indexed by query
+ * slot and stored as 8-bit limbs in tensor-core tiles; the scan is an exact
+ * u8 x u8 -> s32 product on the tensor cores (needs loop_len = N/2, N >= 256).
+ * Replies are identical.  Changing the engine marks every shard unprepared
+ * (call dnspir_fleet_set_shards again) and resets the batch to 1.  Both replace
+ * main_pir_loop (base_pir.rs:1085-1247); the engine choice has no counterpart
+ * in the reference. */
+#define DNSPIR_ENGINE_CUDA_CORES 0
+#define DNSPIR_ENGINE_TENSOR 1
+int dnspir_fleet_set_engine(dnspir_fleet* fleet, int engine);
+/* Tensor engine: time every tile shape for groups of `batch` queries on the
+ * fleet's own shards and keep the fastest for that group size.
+ * ms_per_shape[dnspir_tscan_shapes()] receives each shape's scan time (-1 when
+ * not run); *chosen its index.  No counterpart in the reference. */
+int dnspir_fleet_tune(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
+/* The primary scan alone: the main_pir_loop outputs (base_pir.rs:1085-1247,
+ * reduced) of every shard for nq queries, in groups of the fleet's batch.
+ * Device pointers.  qnat: per query [slot 0 gk0, 1 gk1, 2 query, 3 conjugate
+ * query, 4, 5 unused][factor q1, q2][N] residues in natural NTT order (slot k
+ * = evaluation at zeta^-(2k+1)); out: [query][shard][factor][slot u][lane]
+ * with slot u = (sign, e) for 2k+1 = +-5^e mod 2N, u = sign * N/2 + e. */
+int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, uint32_t* out);
+/* The tensor scan's tile shapes (query-operand rows per CTA, m-tiles per CTA,
+ * pipeline stages); returns their count. */
+int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int max);
 /* Synthetic 2560-byte payloads packed into 10-bit coefficients
  * (pack_bytes_into_coeffs, dns/bucket.rs:289-303): bytes = entries x 2560 on
  * the device, coeffs = entries x 2048 on the device. */

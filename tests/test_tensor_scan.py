@@ -1,0 +1,131 @@
+"""The tensor-core scan (8-bit limbs on tcgen05, tensor layout) against the
+CUDA-core scan and the oracle.
+
+The scan outputs of both engines are compared word for word on the same
+shards and decoded queries (main_pir_loop, base_pir.rs:1085-1247, reduced), and
+full replies of the tensor engine are compared byte for byte with the oracle's
+process_query (pir_wrapper.rs:349-409) and decrypted.
+"""
+import numpy as np
+import pytest
+
+import dnspir_b200 as dp
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+T = orc.T
+P = (67104769, 33550337)
+
+
+def _data(seed, rows, n):
+    return np.random.default_rng(seed).integers(0, T, size=(rows, n), dtype=np.uint16)
+
+
+def _qnat(torch, nq, n, seed):
+    g = np.random.default_rng(seed)
+    q = np.empty((nq, 6, 2, n), dtype=np.uint32)
+    for p in range(2):
+        q[:, :, p, :] = g.integers(0, P[p], size=(nq, 6, n), dtype=np.uint32)
+    return torch.from_numpy(q.view(np.int32)).cuda()
+
+
+def _pair(log2n, l1, l2, count, distinct, seed):
+    n = 1 << log2n
+    data = np.stack([_data(seed + i, 8 * l1, n) for i in range(distinct)])
+    fa = dp.Fleet.general(log2n, l1, l2, count, distinct)
+    fa.set_shards(0, data)
+    fb = dp.Fleet.general(log2n, l1, l2, count, distinct)
+    fb.set_engine(dp.ENGINE_TENSOR)
+    fb.set_shards(0, data)
+    return data, fa, fb
+
+
+def _scan(torch, fleet, q, count, n):
+    out = torch.zeros((q.shape[0], count, 2, n, 8), dtype=torch.int32, device="cuda")
+    fleet.scan(q, out)
+    torch.cuda.synchronize()
+    return out.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("l1,count,distinct", [(256, 1, 1), (128, 2, 2)])
+def test_tensor_scan_equals_cuda_core_scan_n256(l1, count, distinct):
+    torch = pytest.importorskip("torch")
+    n = 256
+    _, fa, fb = _pair(8, l1, 32 if count > 1 else 256, count, distinct, 11 + l1)
+    q = _qnat(torch, 3, n, l1)
+    a = _scan(torch, fa, q, count, n)
+    b = _scan(torch, fb, q, count, n)
+    assert np.array_equal(a, b)
+
+
+@pytest.fixture(scope="module")
+def config1_pair():
+    # 32768 entries: half-size shards (l = 1024 = N/2), 4 shards on 2 distinct
+    l1, l2, shards = dp.get_database_shape(32768)
+    data, fa, fb = _pair(11, l1, l2, shards, 2, 100)
+    refs = []
+    for i in range(2):
+        d = orc.Database(11, l1)
+        d.set_db(data[i])
+        refs.append(d)
+    return data, fa, fb, [refs[k % 2] for k in range(shards)], l1, l2, shards
+
+
+@pytest.mark.parametrize("batch,nq", [(1, 2), (4, 5), (16, 16), (37, 40)])
+def test_tensor_scan_equals_cuda_core_scan_config1(config1_pair, batch, nq):
+    torch = pytest.importorskip("torch")
+    data, fa, fb, refs, l1, l2, shards = config1_pair
+    q = _qnat(torch, nq, 2048, 1000 + batch)
+    a = _scan(torch, fa, q, shards, 2048)
+    fb.set_batch(batch)
+    try:
+        b = _scan(torch, fb, q, shards, 2048)
+    finally:
+        fb.set_batch(1)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("batch", [1, 3, 16])
+def test_tensor_engine_replies_equal_oracle(config1_pair, batch):
+    data, fa, fb, refs, l1, l2, shards = config1_pair
+    rng = orc.Rng(bytes([7, batch]) + bytes(30))
+    qs = [orc.prepare_query(rng, (613 * k + 5) % 8192, k % shards, l1, l2) for k in range(batch + 1)]
+    fb.set_batch(batch)
+    try:
+        got = fb.process_queries([q for q, _ in qs])
+    finally:
+        fb.set_batch(1)
+    for k, ((q, seed), r) in enumerate(zip(qs, got)):
+        assert r == orc.process_query(refs, q), k
+        i, j = (613 * k + 5) % 8192, k % shards
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64))
+
+
+def test_tensor_tune_keeps_results(config1_pair):
+    torch = pytest.importorskip("torch")
+    data, fa, fb, refs, l1, l2, shards = config1_pair
+    chosen, ms, shapes = fb.tune(8)
+    assert 0 <= chosen < len(shapes) and ms[chosen] > 0
+    q = _qnat(torch, 8, 2048, 77)
+    fb.set_batch(8)
+    try:
+        b = _scan(torch, fb, q, shards, 2048)
+    finally:
+        fb.set_batch(1)
+    assert np.array_equal(_scan(torch, fa, q, shards, 2048), b)
+
+
+def test_tensor_engine_shape_rules():
+    # loop_len < N/2 has no tensor layout; an engine change unprepares the shards
+    f = dp.Fleet.general(8, 32, 32, 2, 2)
+    with pytest.raises(dp.DnspirError) as e:
+        f.set_engine(dp.ENGINE_TENSOR)
+    assert e.value.code == 2
+    g = dp.Fleet.general(8, 256, 256, 1, 1)
+    g.set_shards(0, _data(1, 8 * 256, 256)[None])
+    g.set_engine(dp.ENGINE_TENSOR)
+    with pytest.raises(dp.DnspirError) as e:
+        g.perform_double_pir(*([np.zeros(256, dtype=np.uint64)] * 4), np.zeros((2, 256), dtype=np.uint64))
+    assert e.value.code == 7
+    with pytest.raises(dp.DnspirError):
+        g.set_batch(257)
