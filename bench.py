@@ -11,9 +11,16 @@ and logical shard k is served by distinct shard k mod D, as the reference's
 answered, one query per launch sequence (the plain path): decode, scan of all
 256 shards (206 GB), epilogue, secondary database build + key-switch chain,
 reply.  Every answer is decrypted by the client and compared with the stored
-entry.
+entry.  The scan runs on the tensor engine (8-bit limb products on tcgen05)
+unless --engine cuda selects the CUDA-core engine; both give the same replies.
+
+After the plain run, the same fleet answers groups of B queries per pass over
+the slabs (--batched, default 16 and 64; tile shape per B from the autotuner):
+responses/s, p50/p99 per-query latency and the scan's effective GB/s
+(B x slab bytes / scan time) go to the "batched" object of the same line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--engine tensor|cuda] [--batched 16,64]
 
 --gpus N > 1 runs under torchrun: every rank holds a replica of the database
 and answers its own queries (queries are the units; no data-path collective),
@@ -57,6 +64,10 @@ def parse():
     ap.add_argument("--distinct", type=int, default=0, help="distinct shards in HBM (0 = as many as fit)")
     ap.add_argument("--cpu-sample-shards", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--engine", default="tensor", choices=["tensor", "cuda"])
+    ap.add_argument("--batched", default="16,64", help="comma-separated group sizes measured after the plain run")
+    ap.add_argument("--batched-groups", type=int, default=3, help="timed groups per batched size")
+    ap.add_argument("--reserve-gib", type=float, default=22.0, help="HBM left free for workspaces")
     return ap.parse_args()
 
 
@@ -230,12 +241,14 @@ def main():
     per_shard_entries = 8 * l1
     slab_bytes = dp.required_memory_general(11, l1) * 32
     free, _ = torch.cuda.mem_get_info()
-    fit = int((free - (10 << 30)) // slab_bytes)
+    fit = int((free - int(args.reserve_gib * (1 << 30))) // slab_bytes)
     distinct = args.distinct if args.distinct > 0 else max(1, min(shards, fit))
 
     # ---- build and preprocess the fleet on the GPU
     t0 = time.time()
     fleet = dp.Fleet(args.entries, distinct, device=local_rank)
+    if args.engine == "tensor":
+        fleet.set_engine(dp.ENGINE_TENSOR)
     batch = 8
     for first in range(0, distinct, batch):
         cnt = min(batch, distinct - first)
@@ -317,13 +330,73 @@ def main():
               flush=True)
         return 1
 
+    # ---- batched: groups of B queries per pass over the slabs, same fleet
+    batched = {}
+    sizes = [int(x) for x in args.batched.split(",") if x.strip()]
+    if args.engine == "cuda":
+        sizes = [b for b in sizes if b in (1, 2, 4, 8, 16)]
+    if sizes:
+        fleet.set_stream(stream.cuda_stream)
+        pool_n = 2 * max(sizes)
+        pidx = [(int(rng.integers(0, per_shard_entries)), int(rng.integers(0, shards))) for _ in range(pool_n)]
+        pq, pseeds = [], []
+        for k, (i, j) in enumerate(pidx):
+            q, sk = dp.prepare_query(hashlib.sha256(f"client-{rank}-{k}".encode()).digest(), i, j, l1, l2)
+            pq.append(q)
+            pseeds.append(sk)
+        pdev = torch.tensor(np.frombuffer(b"".join(pq), dtype=np.uint8).reshape(pool_n, qlen), device=dev)
+        for B in sizes:
+            shape = None
+            if args.engine == "tensor":
+                ch, tms, shapes = fleet.tune(B)
+                shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
+                         "tuned_ms": round(float(tms[ch]), 3)}
+            fleet.set_batch(B)
+            nq = B * args.batched_groups
+            sel = torch.arange(nq, device=dev) % pool_n
+            qin = pdev[sel].contiguous()
+            rout = torch.zeros((nq, dp.reply_bytes()), dtype=torch.uint8, device=dev)
+            fleet.process_queries_device(qin[:B], rout[:B])  # warm-up group
+            barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fleet.process_queries_device(qin, rout)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            bms = max_over_ranks(e0.elapsed_time(e1))
+            bt = fleet.batch_timings(nq)
+            good = 0
+            host = rout.cpu().numpy()
+            check = list(range(0, nq, max(1, nq // 8)))
+            for k in check:
+                i, j = pidx[k % pool_n]
+                want = pack_host(shard_payload(torch, j % distinct, per_shard_entries, dev)[i].cpu().numpy().tobytes())
+                good += int(np.array_equal(dp.process_reply(host[k].tobytes(), pseeds[k % pool_n]), want))
+            if good != len(check):
+                print(json.dumps({"error": f"batched B={B}: {len(check) - good} of {len(check)} answers failed"}),
+                      flush=True)
+                return 1
+            gscan = [float(bt[3, g * B]) for g in range(args.batched_groups)]
+            batched[str(B)] = {
+                "responses_per_sec": nq * world / (bms * 1e-3), "groups": args.batched_groups,
+                "p50_ms": float(np.median(bt[0])), "p99_ms": float(np.percentile(bt[0], 99)),
+                "scan_ms_per_group": statistics.mean(gscan),
+                "effective_scan_gbs": B * (shards * slab_bytes) / (statistics.mean(gscan) * 1e-3) / 1e9,
+                "secondary_ms_per_group": statistics.mean(float(bt[2, g * B]) for g in range(args.batched_groups)),
+                "tile": shape, "checked": {"decrypted_ok": good, "of": len(check)}}
+        fleet.set_batch(1)
+        fleet.set_stream(None)
+
     # ---- report
     scan_ms = [p[2] for p in phase]
     scan_avg = statistics.mean(scan_ms)
     algo_bytes = shards * slab_bytes + 2 * 4 * dp.N * 4  # slabs + the per-factor query vectors
     achieved = algo_bytes / (scan_avg * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic = profiled_traffic("scan_plain_2p22.md")
+    kname = "tscan_kernel" if args.engine == "tensor" else "scan_batch_kernel"
+    traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_plain_2p22.md")
     value = args.steps * world / (total_ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -344,12 +417,15 @@ def main():
         "unloaded_p50_ms": statistics.median(unloaded) if unloaded else None,
         "primary_ms": statistics.mean(p[0] for p in phase), "secondary_ms": statistics.mean(p[1] for p in phase),
         "scan_ms": scan_avg, "scan_hbm_gbs": achieved, "preprocess_s": prep_s,
-        "roofline": {"kernel": "scan_plain_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "engine": args.engine,
+        "batched": batched,
+        "batched_vs_plain": {b: v["responses_per_sec"] / value for b, v in batched.items()},
+        "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": algo_bytes},
         "e2e": {"value": args.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": qlen,
                 "d2h_bytes_per_step": dp.reply_bytes()},
-        "gpu_launches": 8 * args.steps,
+        "gpu_launches": (9 if args.engine == "tensor" else 8) * args.steps,
         "clocks": clk,
         "checked": {"decrypted_ok": ok, "of": args.steps},
     }

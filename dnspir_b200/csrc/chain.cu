@@ -84,8 +84,12 @@ __device__ __forceinline__ void gs_bf(uint32_t& x, uint32_t& y, uint32_t w, uint
   y = shoup_lazy(d, w, wq, p);
 }
 
-__device__ __forceinline__ void fwd_one(uint32_t* x, int logn, const uint32_t* __restrict__ tw,
-                                        const uint32_t* __restrict__ twq, uint32_t p) {
+// LN vectors `stride` words apart, transformed together: one barrier per pass,
+// and each thread handles the same butterfly group of every vector with its
+// loads issued before the arithmetic (twiddles loaded once).
+template <int LN>
+__device__ __forceinline__ void fwd_multi(uint32_t* x0, int stride, int logn, const uint32_t* __restrict__ tw,
+                                          const uint32_t* __restrict__ twq, uint32_t p) {
   const int N = 1 << logn;
   int s = 0;
   for (; s + 1 < logn; s += 2) {
@@ -94,34 +98,54 @@ __device__ __forceinline__ void fwd_one(uint32_t* x, int logn, const uint32_t* _
     for (int g = threadIdx.x; g < N / 4; g += CT) {
       const int blk = g >> logt2, r = g & (t2 - 1);
       const int j = (blk << (logt2 + 2)) + r;
-      uint32_t x0 = x[j], x1 = x[j + t2], x2 = x[j + t], x3 = x[j + t + t2];
       const uint32_t w = tw[m + blk], wq = twq[m + blk];
-      ct_bf(x0, x2, w, wq, p);
-      ct_bf(x1, x3, w, wq, p);
-      ct_bf(x0, x1, tw[2 * m + 2 * blk], twq[2 * m + 2 * blk], p);
-      ct_bf(x2, x3, tw[2 * m + 2 * blk + 1], twq[2 * m + 2 * blk + 1], p);
-      x[j] = x0;
-      x[j + t2] = x1;
-      x[j + t] = x2;
-      x[j + t + t2] = x3;
+      const uint32_t w1 = tw[2 * m + 2 * blk], w1q = twq[2 * m + 2 * blk];
+      const uint32_t w2 = tw[2 * m + 2 * blk + 1], w2q = twq[2 * m + 2 * blk + 1];
+      uint32_t v[LN][4];
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        const uint32_t* x = x0 + l * stride;
+        v[l][0] = x[j], v[l][1] = x[j + t2], v[l][2] = x[j + t], v[l][3] = x[j + t + t2];
+      }
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        ct_bf(v[l][0], v[l][2], w, wq, p);
+        ct_bf(v[l][1], v[l][3], w, wq, p);
+        ct_bf(v[l][0], v[l][1], w1, w1q, p);
+        ct_bf(v[l][2], v[l][3], w2, w2q, p);
+      }
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        uint32_t* x = x0 + l * stride;
+        x[j] = v[l][0], x[j + t2] = v[l][1], x[j + t] = v[l][2], x[j + t + t2] = v[l][3];
+      }
     }
     __syncthreads();
   }
   if (s < logn) {  // last stage, t = 1
     for (int b = threadIdx.x; b < N / 2; b += CT) {
-      uint32_t u = x[2 * b], v = x[2 * b + 1];
-      ct_bf(u, v, tw[N / 2 + b], twq[N / 2 + b], p);
-      x[2 * b] = u;
-      x[2 * b + 1] = v;
+      const uint32_t w = tw[N / 2 + b], wq = twq[N / 2 + b];
+      uint32_t u[LN], v[LN];
+#pragma unroll
+      for (int l = 0; l < LN; l++) u[l] = x0[l * stride + 2 * b], v[l] = x0[l * stride + 2 * b + 1];
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        ct_bf(u[l], v[l], w, wq, p);
+        x0[l * stride + 2 * b] = red2p(red2p(u[l], 2 * p), p);
+        x0[l * stride + 2 * b + 1] = red2p(red2p(v[l], 2 * p), p);
+      }
     }
-    __syncthreads();
+  } else {
+    for (int b = threadIdx.x; b < N; b += CT)
+#pragma unroll
+      for (int l = 0; l < LN; l++) x0[l * stride + b] = red2p(red2p(x0[l * stride + b], 2 * p), p);
   }
-  for (int b = threadIdx.x; b < N; b += CT) x[b] = red2p(red2p(x[b], 2 * p), p);
   __syncthreads();
 }
 
-__device__ __forceinline__ void inv_one(uint32_t* x, int logn, const uint32_t* __restrict__ tw,
-                                        const uint32_t* __restrict__ twq, uint32_t p) {
+template <int LN>
+__device__ __forceinline__ void inv_multi(uint32_t* x0, int stride, int logn, const uint32_t* __restrict__ tw,
+                                          const uint32_t* __restrict__ twq, uint32_t p) {
   const int N = 1 << logn;
   int s = 0;
   for (; s + 1 < logn; s += 2) {
@@ -130,26 +154,42 @@ __device__ __forceinline__ void inv_one(uint32_t* x, int logn, const uint32_t* _
     for (int g = threadIdx.x; g < N / 4; g += CT) {
       const int blk = g >> s, r = g & (t - 1);
       const int j = (blk << (s + 2)) + r;
-      uint32_t x0 = x[j], x1 = x[j + t], x2 = x[j + 2 * t], x3 = x[j + 3 * t];
-      gs_bf(x0, x1, tw[h0 + 2 * blk], twq[h0 + 2 * blk], p);
-      gs_bf(x2, x3, tw[h0 + 2 * blk + 1], twq[h0 + 2 * blk + 1], p);
+      const uint32_t w0 = tw[h0 + 2 * blk], w0q = twq[h0 + 2 * blk];
+      const uint32_t w1 = tw[h0 + 2 * blk + 1], w1q = twq[h0 + 2 * blk + 1];
       const uint32_t w = tw[h1 + blk], wq = twq[h1 + blk];
-      gs_bf(x0, x2, w, wq, p);
-      gs_bf(x1, x3, w, wq, p);
-      x[j] = x0;
-      x[j + t] = x1;
-      x[j + 2 * t] = x2;
-      x[j + 3 * t] = x3;
+      uint32_t v[LN][4];
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        const uint32_t* x = x0 + l * stride;
+        v[l][0] = x[j], v[l][1] = x[j + t], v[l][2] = x[j + 2 * t], v[l][3] = x[j + 3 * t];
+      }
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        gs_bf(v[l][0], v[l][1], w0, w0q, p);
+        gs_bf(v[l][2], v[l][3], w1, w1q, p);
+        gs_bf(v[l][0], v[l][2], w, wq, p);
+        gs_bf(v[l][1], v[l][3], w, wq, p);
+      }
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        uint32_t* x = x0 + l * stride;
+        x[j] = v[l][0], x[j + t] = v[l][1], x[j + 2 * t] = v[l][2], x[j + 3 * t] = v[l][3];
+      }
     }
     __syncthreads();
   }
   if (s < logn) {  // last stage, t = N/2
     const uint32_t w = tw[1], wq = twq[1];
     for (int j = threadIdx.x; j < N / 2; j += CT) {
-      uint32_t u = x[j], v = x[j + N / 2];
-      gs_bf(u, v, w, wq, p);
-      x[j] = u;
-      x[j + N / 2] = v;
+      uint32_t u[LN], v[LN];
+#pragma unroll
+      for (int l = 0; l < LN; l++) u[l] = x0[l * stride + j], v[l] = x0[l * stride + j + N / 2];
+#pragma unroll
+      for (int l = 0; l < LN; l++) {
+        gs_bf(u[l], v[l], w, wq, p);
+        x0[l * stride + j] = u[l];
+        x0[l * stride + j + N / 2] = v[l];
+      }
     }
     __syncthreads();
   }
@@ -188,14 +228,13 @@ struct ChainArgs {
   uint32_t c_first, cinv_first, inv5;
 };
 
-// Shared-memory plan (u32 words, N = 2^logn):
+// Primary chain (preprocessing), one lane per block.  Shared-memory plan (u32
+// words, N = 2^logn):
 //   A, TC, D           N each    state a, saved sigma_5(a), work vector
 //   X[2]               2N        iNTT outputs published to the peer block
 //   CG0, CG1, CQA      3N        gk_a0 R, gk_a1 R, qry_a R of this factor and half
 //   FW, FWQ, IW, IWQ   4N        twiddles of this factor
-//   B, QG0, QG1, QQB   4N        b, gk_b0 R, gk_b1 R, qry_b R (secondary only)
-template <bool SECONDARY>
-__device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, int q, int s, uint32_t* sm) {
+__device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane, int s, uint32_t* sm) {
   cg::cluster_group cluster = cg::this_cluster();
   const int p = (int)cluster.block_rank();
   const int logn = a.g.log2n;
@@ -214,23 +253,12 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
   uint32_t* FWQ = FW + N;
   uint32_t* IW = FWQ + N;
   uint32_t* IWQ = IW + N;
-  uint32_t* B = IWQ + N;
-  uint32_t* QG0 = B + N;
-  uint32_t* QG1 = QG0 + N;
-  uint32_t* QQB = QG1 + N;
   for (int b = threadIdx.x; b < N; b += CT) {
     A[b] = 0;
-    if (SECONDARY) B[b] = 0;
     const size_t o = (size_t)p * N + b;
     CG0[b] = mont_reduce((uint64_t)a.gka[o] * cp.r2, pr, cp.pinv);
     CG1[b] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
     CQA[b] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, pr, cp.pinv);
-    if (SECONDARY) {
-      const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
-      QG0[b] = mont_reduce((uint64_t)qq[o] * cp.r2, pr, cp.pinv);
-      QG1[b] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
-      QQB[b] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, pr, cp.pinv);
-    }
     FW[b] = a.T.fw[p][b];
     FWQ[b] = a.T.fwq[p][b];
     IW[b] = a.T.iw[p][b];
@@ -238,7 +266,7 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
   }
   cluster.sync();
   uint32_t* peerX = cluster.map_shared_rank(X, p ^ 1);
-  uint32_t* slab = SECONDARY ? nullptr : a.slabs[s];
+  uint32_t* slab = a.slabs[s];
   uint32_t ci = a.c_first, cinv = a.cinv_first;
   constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
   for (uint32_t i = 0; i < a.g.L; i++) {
@@ -249,24 +277,17 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
       const int pos = threadIdx.x + c * CT;
       e[c] = 0;
       if (pos < N) {
-        if (SECONDARY) {
-          e[c] = __ldg(a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + lane) * N + pos);
-        } else {
-          const uint32_t j = brv(pos, logn);
-          const uint32_t ks = gidx(cinv * (2 * j + 1), mask);
-          e[c] = slab[slab_off(a.g, p, h, i, 0, __ldg(a.maps.uof + ks)) + lane];
-        }
+        const uint32_t j = brv(pos, logn);
+        const uint32_t ks = gidx(cinv * (2 * j + 1), mask);
+        e[c] = slab[slab_off(a.g, p, h, i, 0, __ldg(a.maps.uof + ks)) + lane];
       }
     }
-    // sigma_5 on a (and b)
-    uint32_t ra[PER], rb[PER];
+    // sigma_5 on a
+    uint32_t ra[PER];
 #pragma unroll
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
-      if (pos < N) {
-        ra[c] = A[pos];
-        if (SECONDARY) rb[c] = B[pos];
-      }
+      if (pos < N) ra[c] = A[pos];
     }
     __syncthreads();
 #pragma unroll
@@ -276,11 +297,10 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
         const uint32_t dst = __ldg(a.galb + pos);
         TC[dst] = ra[c];
         D[dst] = ra[c];
-        if (SECONDARY) B[dst] = rb[c];
       }
     }
     __syncthreads();
-    inv_one(D, logn, IW, IWQ, pr);
+    inv_multi<1>(D, 0, logn, IW, IWQ, pr);
     uint32_t* Xc = X + (i & 1) * N;
     for (int b = threadIdx.x; b < N; b += CT) Xc[b] = D[b];
     cluster.sync();
@@ -291,7 +311,7 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
       D[b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
     }
     __syncthreads();
-    fwd_one(D, logn, FW, FWQ, pr);
+    fwd_multi<1>(D, 0, logn, FW, FWQ, pr);
 #pragma unroll
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
@@ -300,55 +320,169 @@ __device__ __forceinline__ void chain_body(const ChainArgs& a, int h, int lane, 
         const uint32_t n0 = sub_mod(TC[pos], mont_reduce((uint64_t)n1 * cp.c26, pr, cp.pinv), pr);
         A[pos] = mont_reduce((uint64_t)n0 * CG0[pos] + (uint64_t)n1 * CG1[pos] + (uint64_t)e[c] * CQA[pos], pr,
                              cp.pinv);
-        if (SECONDARY) {
-          B[pos] = mont_reduce(((uint64_t)B[pos] << 32) + (uint64_t)n0 * QG0[pos] + (uint64_t)n1 * QG1[pos] +
-                                   (uint64_t)e[c] * QQB[pos],
-                               pr, cp.pinv);
-        } else {
-          TC[pos] = n0;
+        TC[pos] = n0;
+      }
+    }
+    __syncthreads();
+    // key digits of row i in the scan layout: position u (natural slot k with
+    // 2k+1 = g[u]) holds G_i[idx(5^(L-1-i) g[u])]
+    for (int u = threadIdx.x; u < N; u += CT) {
+      const uint32_t jb = brv(gidx(ci * __ldg(a.maps.g + u), mask), logn);
+      slab[slab_off(a.g, p, h, i, 1, u) + lane] = TC[jb];
+      slab[slab_off(a.g, p, h, i, 2, u) + lane] = D[jb];
+    }
+    // TC and D are rewritten only after the next step's first barrier
+    ci = (ci * a.inv5) & mask;
+    cinv = (cinv * 5) & mask;
+  }
+  uint32_t* o = a.a_out + (((size_t)s * a.g.H + h) * SIMD + lane) * 2 * N;
+  for (int b = threadIdx.x; b < N; b += CT) o[(size_t)p * N + b] = A[b];
+  cluster.sync();  // keep this block's shared memory alive until the peer's last read
+}
+
+// Secondary chain: the three parts of one query's secondary ciphertext at half
+// h in one block (factor p = rank in the cluster), so that each transform pass
+// and each cluster barrier serves three vectors.  Shared memory (u32 words):
+//   CG0 CG1 CQA QG0 QG1 QQB   6N   gk_a0, gk_a1, qry_a, gk_b0, gk_b1, qry_b (Montgomery form)
+//   FW FWQ IW IWQ             4N   twiddles of this factor
+//   per part: A TC D X0 X1 B  6N   a, saved sigma_5(a), work vector, published iNTT x2, b
+// 28N words = 224 KiB at N = 2048: one block per SM.
+constexpr int SEC_PART_WORDS = 6;  // x N
+constexpr int SEC_SMEM_WORDS = 10 + CTXT_PARTS * SEC_PART_WORDS;  // x N
+
+__device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q, uint32_t* sm) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int p = (int)cluster.block_rank();
+  const int logn = a.g.log2n;
+  const int N = 1 << logn;
+  const ChainPrime cp = a.cp[p];
+  const uint32_t pr = cp.p;
+  uint32_t* CG0 = sm;
+  uint32_t* CG1 = CG0 + N;
+  uint32_t* CQA = CG1 + N;
+  uint32_t* QG0 = CQA + N;
+  uint32_t* QG1 = QG0 + N;
+  uint32_t* QQB = QG1 + N;
+  uint32_t* FW = QQB + N;
+  uint32_t* FWQ = FW + N;
+  uint32_t* IW = FWQ + N;
+  uint32_t* IWQ = IW + N;
+  uint32_t* P0 = IWQ + N;  // part blocks
+  const int PS = SEC_PART_WORDS * N;
+  const int oTC = N, oD = 2 * N, oX = 3 * N, oB = 5 * N;
+  const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
+  for (int b = threadIdx.x; b < N; b += CT) {
+    const size_t o = (size_t)p * N + b;
+    CG0[b] = mont_reduce((uint64_t)a.gka[o] * cp.r2, pr, cp.pinv);
+    CG1[b] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
+    CQA[b] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, pr, cp.pinv);
+    QG0[b] = mont_reduce((uint64_t)qq[o] * cp.r2, pr, cp.pinv);
+    QG1[b] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
+    QQB[b] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, pr, cp.pinv);
+    FW[b] = a.T.fw[p][b];
+    FWQ[b] = a.T.fwq[p][b];
+    IW[b] = a.T.iw[p][b];
+    IWQ[b] = a.T.iwq[p][b];
+#pragma unroll
+    for (int t = 0; t < CTXT_PARTS; t++) {
+      P0[t * PS + b] = 0;
+      P0[t * PS + oB + b] = 0;
+    }
+  }
+  cluster.sync();
+  const uint32_t* peer = cluster.map_shared_rank(P0, p ^ 1);
+  constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
+  for (uint32_t i = 0; i < a.g.L; i++) {
+    // entries of row i (the three parts' lanes are adjacent), consumed at the end of the step
+    const uint32_t* Ei = a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + (size_t)q * CTXT_PARTS) * N;
+    uint32_t e[CTXT_PARTS][PER], ra[CTXT_PARTS][PER], rb[CTXT_PARTS][PER];
+#pragma unroll
+    for (int t = 0; t < CTXT_PARTS; t++)
+#pragma unroll
+      for (int c = 0; c < PER; c++) {
+        const int pos = threadIdx.x + c * CT;
+        e[t][c] = pos < N ? __ldg(Ei + (size_t)t * N + pos) : 0;
+        if (pos < N) {
+          ra[t][c] = P0[t * PS + pos];
+          rb[t][c] = P0[t * PS + oB + pos];
+        }
+      }
+    __syncthreads();
+    // sigma_5 on a and b
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      if (pos < N) {
+        const uint32_t dst = __ldg(a.galb + pos);
+#pragma unroll
+        for (int t = 0; t < CTXT_PARTS; t++) {
+          P0[t * PS + oTC + dst] = ra[t][c];
+          P0[t * PS + oD + dst] = ra[t][c];
+          P0[t * PS + oB + dst] = rb[t][c];
         }
       }
     }
     __syncthreads();
-    if (!SECONDARY) {
-      // key digits of row i in the scan layout: position u (natural slot k with
-      // 2k+1 = g[u]) holds G_i[idx(5^(L-1-i) g[u])]
-      for (int u = threadIdx.x; u < N; u += CT) {
-        const uint32_t jb = brv(gidx(ci * __ldg(a.maps.g + u), mask), logn);
-        slab[slab_off(a.g, p, h, i, 1, u) + lane] = TC[jb];
-        slab[slab_off(a.g, p, h, i, 2, u) + lane] = D[jb];
-      }
-      // TC and D are rewritten only after the next step's first barrier
-      ci = (ci * a.inv5) & mask;
-      cinv = (cinv * 5) & mask;
-    }
-  }
-  if (SECONDARY) {
-    uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + lane % CTXT_PARTS) * 2) * 2 * N;
+    inv_multi<CTXT_PARTS>(P0 + oD, PS, logn, IW, IWQ, pr);
+    const int xo = oX + (int)(i & 1) * N;
+    for (int b = threadIdx.x; b < N; b += CT)
+#pragma unroll
+      for (int t = 0; t < CTXT_PARTS; t++) P0[t * PS + xo + b] = P0[t * PS + oD + b];
+    cluster.sync();
     for (int b = threadIdx.x; b < N; b += CT) {
-      o[(size_t)p * N + b] = A[b];
-      o[2 * (size_t)N + (size_t)p * N + b] = B[b];
+      uint32_t own[CTXT_PARTS], other[CTXT_PARTS];
+#pragma unroll
+      for (int t = 0; t < CTXT_PARTS; t++) own[t] = P0[t * PS + oD + b], other[t] = peer[t * PS + xo + b];
+#pragma unroll
+      for (int t = 0; t < CTXT_PARTS; t++) {
+        const int32_t hd = p == 0 ? high_digit(own[t], other[t], a.cp[0], a.cp[1])
+                                  : high_digit(other[t], own[t], a.cp[0], a.cp[1]);
+        P0[t * PS + oD + b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
+      }
     }
-  } else {
-    uint32_t* o = a.a_out + (((size_t)s * a.g.H + h) * SIMD + lane) * 2 * N;
-    for (int b = threadIdx.x; b < N; b += CT) o[(size_t)p * N + b] = A[b];
+    __syncthreads();
+    fwd_multi<CTXT_PARTS>(P0 + oD, PS, logn, FW, FWQ, pr);
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      if (pos < N) {
+        const uint32_t cg0 = CG0[pos], cg1 = CG1[pos], cqa = CQA[pos];
+        const uint32_t qg0 = QG0[pos], qg1 = QG1[pos], qqb = QQB[pos];
+#pragma unroll
+        for (int t = 0; t < CTXT_PARTS; t++) {
+          uint32_t* P = P0 + t * PS;
+          const uint32_t n1 = P[oD + pos];
+          const uint32_t n0 = sub_mod(P[oTC + pos], mont_reduce((uint64_t)n1 * cp.c26, pr, cp.pinv), pr);
+          P[pos] = mont_reduce((uint64_t)n0 * cg0 + (uint64_t)n1 * cg1 + (uint64_t)e[t][c] * cqa, pr, cp.pinv);
+          P[oB + pos] = mont_reduce(((uint64_t)P[oB + pos] << 32) + (uint64_t)n0 * qg0 + (uint64_t)n1 * qg1 +
+                                        (uint64_t)e[t][c] * qqb,
+                                    pr, cp.pinv);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int bb = threadIdx.x; bb < CTXT_PARTS * N; bb += CT) {
+    const int t = bb >> logn, b = bb & (N - 1);
+    uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + t) * 2) * 2 * N;
+    o[(size_t)p * N + b] = P0[t * PS + b];
+    o[2 * (size_t)N + (size_t)p * N + b] = P0[t * PS + oB + b];
   }
   cluster.sync();  // keep this block's shared memory alive until the peer's last read
 }
 
-// grid: x = factor (cluster of 2), y = part * H + half, z = query
+// grid: x = factor (cluster of 2), y = half, z = query
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT)
     secondary_chain_kernel(ChainArgs a) {
   extern __shared__ uint32_t sm[];
-  const int h = blockIdx.y % a.g.H, part = blockIdx.y / a.g.H, q = blockIdx.z;
-  chain_body<true>(a, h, q * CTXT_PARTS + part, q, 0, sm);
+  secondary_body(a, blockIdx.y, blockIdx.z, sm);
 }
 
 // grid: x = factor (cluster of 2), y = lane * H + half, z = shard
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT) primary_chain_kernel(ChainArgs a) {
   extern __shared__ uint32_t sm[];
   const int h = blockIdx.y % a.g.H, lane = blockIdx.y / a.g.H;
-  chain_body<false>(a, h, lane, 0, blockIdx.z, sm);
+  primary_body(a, h, lane, blockIdx.z, sm);
 }
 
 // reply_a = a_main + a_conj -> iNTT -> CRT; also the 17-bit mod switch
@@ -424,7 +558,9 @@ static ChainArgs chain_args(const Group& g, const ChainConsts& cc, const NttTabl
   return a;
 }
 
-static size_t chain_smem(const Group& g, bool secondary) { return (size_t)(secondary ? 16 : 12) * g.n * 4; }
+static size_t chain_smem(const Group& g, bool secondary) {
+  return (size_t)(secondary ? SEC_SMEM_WORDS : 12) * g.n * 4;
+}
 
 void launch_primary_chain(uint32_t* const* slabs_dev, int nshards, uint32_t* a_out, const Group& g,
                           const ChainConsts& cc, const NttTables& T, cudaStream_t st) {
@@ -458,7 +594,7 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   a.out = out;
   const size_t smem = chain_smem(g, true);
   set_smem(secondary_chain_kernel, smem);
-  dim3 grid(2, CTXT_PARTS * g.H, nq);
+  dim3 grid(2, g.H, nq);
   secondary_chain_kernel<<<grid, CT, smem, st>>>(a);
 }
 

@@ -4,8 +4,8 @@
 //
 // Queries are answered in groups of up to `batch`: one pass of the scan over
 // every shard serves the whole group (the slab is read once per group), then
-// the secondary databases are encoded and evaluated in chunks of up to 16
-// queries.  Two scan engines: CUDA cores over the lane layout (groups of 1, 2,
+// the secondary databases are encoded and evaluated in chunks of one wave of
+// chain clusters (SMs / (2 H) queries, capped by a memory budget).  Two scan engines: CUDA cores over the lane layout (groups of 1, 2,
 // 4, 8 or 16) and the tensor cores over the tensor layout (groups up to 256,
 // tile shape per group size from a table or from dnspir_fleet_tune).
 // Two buffer slots alternate between groups: the primary phase of group k+1
@@ -47,6 +47,7 @@ struct dnspir_fleet {
   DBuf secE, chain_out, qzq, reply_zq;  // used by one stream at a time
   HBuf rpin;                            // host staging of the replies of one call
   int batch = 1;
+  int sec_chunk = 1;  // queries per secondary launch sequence
   int engine = DNSPIR_ENGINE_CUDA_CORES;
   DBuf qb, err_word, tmp_lane;      // tensor engine: query operand, wait-error word, preprocessing scratch
   std::map<int, int> tuned;         // tensor engine: group size -> tile shape index
@@ -70,7 +71,7 @@ struct dnspir_fleet {
 namespace {
 
 const size_t QV_WORDS_PER_QUERY = 6 * 2;  // decoded slots x factors, times N
-const int SEC_CHUNK = 16;                 // queries per secondary launch sequence
+const size_t SEC_BUDGET = (size_t)6 << 30;  // secondary workspace of one chunk
 const int TENSOR_MAX_BATCH = 256;
 
 // Tile shape of the tensor scan for a group of nb queries, and the padded
@@ -157,7 +158,7 @@ int stage_primary(dnspir_fleet* f, QSlot& s, int nb, int Bk, cudaEvent_t* t) {
   }
   CK(cudaEventRecord(t[2], st));
   launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
-                          s.sec_in.as<uint16_t>(), SEC_CHUNK, g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, st);
+                          s.sec_in.as<uint16_t>(), f->sec_chunk, g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, st);
   CK(cudaEventRecord(t[3], st));
   CK(cudaEventRecord(s.prim_done, st));
   s.prim_recorded = true;
@@ -173,24 +174,26 @@ int stage_secondary(dnspir_fleet* f, QSlot& s, int nb, cudaEvent_t* t, uint8_t* 
                     uint64_t* reply_zq, uint8_t* host_reply) {
   const Group& g2 = f->g2;
   const size_t n = g2.n;
-  const int cmax = std::min(nb, SEC_CHUNK);
+  const int cmax = std::min(nb, f->sec_chunk);
   const int nlmax = CTXT_PARTS * cmax;
   cudaStream_t st = f->sec;
-  CKR(f->ws.A.ensure((size_t)g2.l * nlmax * n * 4));
+  // the encoder's column transforms (A) are dead before the lift writes secE:
+  // A lives at the start of secE's buffer
+  const size_t a_bytes = (size_t)g2.l * nlmax * n * 4, e_bytes = (size_t)2 * g2.H * g2.L * nlmax * n * 4;
   CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * nlmax * n * 4));
-  CKR(f->secE.ensure((size_t)2 * g2.H * g2.L * nlmax * n * 4));
+  CKR(f->secE.ensure(std::max(a_bytes, e_bytes)));
   CKR(f->chain_out.ensure((size_t)cmax * g2.H * CTXT_PARTS * 2 * 2 * n * 4));
   CK(cudaStreamWaitEvent(st, s.prim_done, 0));
   CK(cudaEventRecord(t[4], st));
   const uint32_t l_in = f->S * SIMD;
   const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
   const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
-  for (int c0 = 0; c0 < nb; c0 += SEC_CHUNK) {
-    const int nc = std::min(SEC_CHUNK, nb - c0);
+  for (int c0 = 0; c0 < nb; c0 += f->sec_chunk) {
+    const int nc = std::min(f->sec_chunk, nb - c0);
     const int nl = CTXT_PARTS * nc;
     const uint16_t* in = s.sec_in.as<uint16_t>() + (size_t)c0 * CTXT_PARTS * l_in * n;
-    launch_encode_cols(in, f->ws.A.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
-    launch_encode_rows(f->ws.A.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
+    launch_encode_cols(in, f->secE.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
+    launch_encode_rows(f->secE.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
     launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, nl, 1, maps, f->ctx->T, st);
     launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>() + (size_t)c0 * QV_WORDS_PER_QUERY * n,
                            QV_WORDS_PER_QUERY * n, nc, f->chain_out.as<uint32_t>(), g2, cc, f->ctx->T, st);
@@ -270,6 +273,15 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   f->g2 = make_group(log2_n, secondary_order);
   f->S = num_shards;
   f->D = num_distinct;
+  {
+    // one wave of secondary chain clusters (one block per SM, 2 H per query)
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const Group& g2 = f->g2;
+    const size_t per_query = ((size_t)2 * g2.H * g2.L + (size_t)g2.H * g2.L) * CTXT_PARTS * g2.n * 4;
+    const int wave = std::max(1, sms / (2 * (int)g2.H));
+    f->sec_chunk = (int)std::max<size_t>(1, std::min<size_t>(wave, SEC_BUDGET / per_query));
+  }
   CK(cudaStreamCreateWithFlags(&f->own, cudaStreamNonBlocking));
   {
     // the secondary phase runs at the highest priority so that its few,
