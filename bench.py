@@ -15,12 +15,12 @@ entry.  The scan runs on the tensor engine (8-bit limb products on tcgen05)
 unless --engine cuda selects the CUDA-core engine; both give the same replies.
 
 After the plain run, the same fleet answers groups of B queries per pass over
-the slabs (--batched, default 16 and 64; tile shape per B from the autotuner):
+the slabs (--batched, default 16, 64 and 128; tile shape per B from the autotuner):
 responses/s, p50/p99 per-query latency and the scan's effective GB/s
 (B x slab bytes / scan time) go to the "batched" object of the same line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--engine tensor|cuda] [--batched 16,64]
+                  [--engine tensor|cuda] [--batched 16,64,128]
 
 --gpus N > 1 runs under torchrun: every rank holds a replica of the database
 and answers its own queries (queries are the units; no data-path collective),
@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--cpu-sample-shards", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--engine", default="tensor", choices=["tensor", "cuda"])
-    ap.add_argument("--batched", default="16,64", help="comma-separated group sizes measured after the plain run")
+    ap.add_argument("--batched", default="16,64,128", help="comma-separated group sizes measured after the plain run")
     ap.add_argument("--batched-groups", type=int, default=3, help="timed groups per batched size")
     ap.add_argument("--reserve-gib", type=float, default=22.0, help="HBM left free for workspaces")
     return ap.parse_args()

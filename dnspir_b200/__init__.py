@@ -89,6 +89,17 @@ def lib():
         L.dnspir_fleet_tune.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_tscan_shapes.argtypes = [_vp, _vp, _vp, c.c_int]
         L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
+        L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
+        L.dnspir_server_add_db.argtypes = [_vp, _vp, c.c_uint32, _u32p]
+        L.dnspir_server_start.argtypes = [_vp, c.c_int]
+        L.dnspir_server_open_session.argtypes = [_vp, c.c_char_p, c.c_uint64, _u64p]
+        L.dnspir_server_close_session.argtypes = [_vp, c.c_uint64]
+        L.dnspir_server_submit.argtypes = [_vp, c.c_uint32, c.c_int64, c.c_char_p, c.c_uint64, _u64p]
+        L.dnspir_server_poll.argtypes = [_vp, c.c_uint64, _vp, c.c_uint64, c.POINTER(c.c_int)]
+        L.dnspir_server_wait.argtypes = [_vp, c.c_uint64, _vp, c.c_uint64, c.c_uint32]
+        L.dnspir_server_db_stats.argtypes = [_vp, c.c_uint32, _u64p, _u32p, _u64p, _u64p, _vp, c.c_uint32, _u32p]
+        L.dnspir_server_stop.argtypes = [_vp]
+        L.dnspir_server_destroy.argtypes = [_vp]
         L.dnspir_fleet_batch_timings.argtypes = [_vp, c.c_uint32] + [_vp] * 4
         L.dnspir_fleet_slab_bytes.restype = c.c_uint64
         L.dnspir_fleet_slab_bytes.argtypes = [_vp]
@@ -389,3 +400,73 @@ class Fleet:
     @property
     def slab_bytes(self):
         return lib().dnspir_fleet_slab_bytes(self._h)
+
+
+GALOIS_KEY_BYTES = 2 * N * 50 // 8
+
+
+class Server:
+    """Serving loop over resident fleets (continuous batching, CUDA graphs,
+    device-resident client sessions).  Fleets stay attached until stop()."""
+
+    def __init__(self, max_sessions=0, device=0):
+        h = _vp()
+        _check(lib().dnspir_server_create(device, max_sessions, ctypes.byref(h)))
+        self._h = h
+        self._fleets = []
+
+    def add_db(self, fleet, max_batch):
+        i = ctypes.c_uint32()
+        _check(lib().dnspir_server_add_db(self._h, fleet._h, max_batch, ctypes.byref(i)))
+        self._fleets.append(fleet)
+        return i.value
+
+    def start(self, graphs=True):
+        _check(lib().dnspir_server_start(self._h, 1 if graphs else 0))
+
+    def open_session(self, galois_key_bytes):
+        s = ctypes.c_uint64()
+        b = bytes(galois_key_bytes)
+        _check(lib().dnspir_server_open_session(self._h, b, len(b), ctypes.byref(s)))
+        return s.value
+
+    def close_session(self, session):
+        _check(lib().dnspir_server_close_session(self._h, session))
+
+    def submit(self, db, query, session=-1):
+        t = ctypes.c_uint64()
+        b = bytes(query)
+        _check(lib().dnspir_server_submit(self._h, db, session, b, len(b), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        out = np.zeros(reply_bytes(), dtype=np.uint8)
+        done = ctypes.c_int()
+        _check(lib().dnspir_server_poll(self._h, ticket, _ptr(out), out.size, ctypes.byref(done)))
+        return out.tobytes() if done.value else None
+
+    def wait(self, ticket, timeout_ms=120000):
+        out = np.zeros(reply_bytes(), dtype=np.uint8)
+        _check(lib().dnspir_server_wait(self._h, ticket, _ptr(out), out.size, timeout_ms))
+        return out.tobytes()
+
+    def stats(self, db, max_latencies=1 << 20):
+        comp, adm, grp, ggrp, n = (ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint64(),
+                                   ctypes.c_uint32())
+        lat = np.zeros(max_latencies)
+        _check(lib().dnspir_server_db_stats(self._h, db, ctypes.byref(comp), ctypes.byref(adm), ctypes.byref(grp),
+                                            ctypes.byref(ggrp), _ptr(lat), max_latencies, ctypes.byref(n)))
+        return {"completed": comp.value, "admitted_batch": adm.value, "groups": grp.value,
+                "graph_groups": ggrp.value, "latencies_ms": lat[:n.value].copy()}
+
+    def stop(self):
+        if getattr(self, "_h", None):
+            _check(lib().dnspir_server_stop(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.dnspir_server_destroy(self._h)
+            self._h = None
+            self._fleets = []
+
+    __del__ = close

@@ -5,7 +5,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = ["api.cu", "fleet.cu", "encode.cu", "chain.cu", "scan.cu", "tscan.cu", "wire.cu", "client.cpp", "noalloc.cu"]
+SRC = ["api.cu", "fleet.cu", "encode.cu", "chain.cu", "scan.cu", "tscan.cu", "server.cu", "wire.cu", "client.cpp", "noalloc.cu"]
 OUT = os.path.join(HERE, "libdnspir_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -20,7 +20,7 @@ FLAGS = [
 def build(verbose=False, extra=()):
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
     newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(HERE, "csrc", h) for h in
-                                                   ("common.cuh", "ntt.cuh", "kernels.cuh", "host.h")] +
+                                                   ("common.cuh", "ntt.cuh", "kernels.cuh", "host.h", "fleet_impl.h")] +
                  [os.path.join(ROOT, "include", "dnspir.h")])
     if os.path.exists(OUT) and os.path.getmtime(OUT) >= newest and not extra:
         return OUT

@@ -340,17 +340,21 @@ __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane
   cluster.sync();  // keep this block's shared memory alive until the peer's last read
 }
 
-// Secondary chain: the three parts of one query's secondary ciphertext at half
-// h in one block (factor p = rank in the cluster), so that each transform pass
-// and each cluster barrier serves three vectors.  Shared memory (u32 words):
+// Secondary chain: LN of the three parts of one query's secondary ciphertext
+// at half h in one block (factor p = rank in the cluster), parts part0 ..
+// part0 + LN - 1.  With LN = 3 each transform pass and cluster barrier serves
+// three vectors (throughput: one wave holds SMs / (2 H) queries); with LN = 1
+// the block needs 128 KiB and shares an SM with a scan block (latency: the
+// chains of a few queries overlap the next scan).  Shared memory (u32 words):
 //   CG0 CG1 CQA QG0 QG1 QQB   6N   gk_a0, gk_a1, qry_a, gk_b0, gk_b1, qry_b (Montgomery form)
 //   FW FWQ IW IWQ             4N   twiddles of this factor
 //   per part: A TC D X0 X1 B  6N   a, saved sigma_5(a), work vector, published iNTT x2, b
-// 28N words = 224 KiB at N = 2048: one block per SM.
+// (10 + 6 LN) N words: 224 KiB for LN = 3, 128 KiB for LN = 1 at N = 2048.
 constexpr int SEC_PART_WORDS = 6;  // x N
-constexpr int SEC_SMEM_WORDS = 10 + CTXT_PARTS * SEC_PART_WORDS;  // x N
+__host__ __device__ constexpr int sec_smem_words(int ln) { return 10 + ln * SEC_PART_WORDS; }
 
-__device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q, uint32_t* sm) {
+template <int LN>
+__device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q, int part0, uint32_t* sm) {
   cg::cluster_group cluster = cg::this_cluster();
   const int p = (int)cluster.block_rank();
   const int logn = a.g.log2n;
@@ -384,7 +388,7 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
     IW[b] = a.T.iw[p][b];
     IWQ[b] = a.T.iwq[p][b];
 #pragma unroll
-    for (int t = 0; t < CTXT_PARTS; t++) {
+    for (int t = 0; t < LN; t++) {
       P0[t * PS + b] = 0;
       P0[t * PS + oB + b] = 0;
     }
@@ -394,10 +398,10 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
   constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
   for (uint32_t i = 0; i < a.g.L; i++) {
     // entries of row i (the three parts' lanes are adjacent), consumed at the end of the step
-    const uint32_t* Ei = a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + (size_t)q * CTXT_PARTS) * N;
-    uint32_t e[CTXT_PARTS][PER], ra[CTXT_PARTS][PER], rb[CTXT_PARTS][PER];
+    const uint32_t* Ei = a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + (size_t)q * CTXT_PARTS + part0) * N;
+    uint32_t e[LN][PER], ra[LN][PER], rb[LN][PER];
 #pragma unroll
-    for (int t = 0; t < CTXT_PARTS; t++)
+    for (int t = 0; t < LN; t++)
 #pragma unroll
       for (int c = 0; c < PER; c++) {
         const int pos = threadIdx.x + c * CT;
@@ -415,7 +419,7 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
       if (pos < N) {
         const uint32_t dst = __ldg(a.galb + pos);
 #pragma unroll
-        for (int t = 0; t < CTXT_PARTS; t++) {
+        for (int t = 0; t < LN; t++) {
           P0[t * PS + oTC + dst] = ra[t][c];
           P0[t * PS + oD + dst] = ra[t][c];
           P0[t * PS + oB + dst] = rb[t][c];
@@ -423,25 +427,25 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
       }
     }
     __syncthreads();
-    inv_multi<CTXT_PARTS>(P0 + oD, PS, logn, IW, IWQ, pr);
+    inv_multi<LN>(P0 + oD, PS, logn, IW, IWQ, pr);
     const int xo = oX + (int)(i & 1) * N;
     for (int b = threadIdx.x; b < N; b += CT)
 #pragma unroll
-      for (int t = 0; t < CTXT_PARTS; t++) P0[t * PS + xo + b] = P0[t * PS + oD + b];
+      for (int t = 0; t < LN; t++) P0[t * PS + xo + b] = P0[t * PS + oD + b];
     cluster.sync();
     for (int b = threadIdx.x; b < N; b += CT) {
-      uint32_t own[CTXT_PARTS], other[CTXT_PARTS];
+      uint32_t own[LN], other[LN];
 #pragma unroll
-      for (int t = 0; t < CTXT_PARTS; t++) own[t] = P0[t * PS + oD + b], other[t] = peer[t * PS + xo + b];
+      for (int t = 0; t < LN; t++) own[t] = P0[t * PS + oD + b], other[t] = peer[t * PS + xo + b];
 #pragma unroll
-      for (int t = 0; t < CTXT_PARTS; t++) {
+      for (int t = 0; t < LN; t++) {
         const int32_t hd = p == 0 ? high_digit(own[t], other[t], a.cp[0], a.cp[1])
                                   : high_digit(other[t], own[t], a.cp[0], a.cp[1]);
         P0[t * PS + oD + b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
       }
     }
     __syncthreads();
-    fwd_multi<CTXT_PARTS>(P0 + oD, PS, logn, FW, FWQ, pr);
+    fwd_multi<LN>(P0 + oD, PS, logn, FW, FWQ, pr);
 #pragma unroll
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
@@ -449,7 +453,7 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
         const uint32_t cg0 = CG0[pos], cg1 = CG1[pos], cqa = CQA[pos];
         const uint32_t qg0 = QG0[pos], qg1 = QG1[pos], qqb = QQB[pos];
 #pragma unroll
-        for (int t = 0; t < CTXT_PARTS; t++) {
+        for (int t = 0; t < LN; t++) {
           uint32_t* P = P0 + t * PS;
           const uint32_t n1 = P[oD + pos];
           const uint32_t n0 = sub_mod(P[oTC + pos], mont_reduce((uint64_t)n1 * cp.c26, pr, cp.pinv), pr);
@@ -462,20 +466,20 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
     }
     __syncthreads();
   }
-  for (int bb = threadIdx.x; bb < CTXT_PARTS * N; bb += CT) {
+  for (int bb = threadIdx.x; bb < LN * N; bb += CT) {
     const int t = bb >> logn, b = bb & (N - 1);
-    uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + t) * 2) * 2 * N;
+    uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + part0 + t) * 2) * 2 * N;
     o[(size_t)p * N + b] = P0[t * PS + b];
     o[2 * (size_t)N + (size_t)p * N + b] = P0[t * PS + oB + b];
   }
   cluster.sync();  // keep this block's shared memory alive until the peer's last read
 }
 
-// grid: x = factor (cluster of 2), y = half, z = query
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT)
-    secondary_chain_kernel(ChainArgs a) {
+// grid: x = factor (cluster of 2), y = (part group) * H + half, z = query
+template <int LN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT) secondary_chain_kernel(ChainArgs a) {
   extern __shared__ uint32_t sm[];
-  secondary_body(a, blockIdx.y, blockIdx.z, sm);
+  secondary_body<LN>(a, blockIdx.y % a.g.H, blockIdx.z, (blockIdx.y / a.g.H) * LN, sm);
 }
 
 // grid: x = factor (cluster of 2), y = lane * H + half, z = shard
@@ -558,8 +562,8 @@ static ChainArgs chain_args(const Group& g, const ChainConsts& cc, const NttTabl
   return a;
 }
 
-static size_t chain_smem(const Group& g, bool secondary) {
-  return (size_t)(secondary ? SEC_SMEM_WORDS : 12) * g.n * 4;
+static size_t chain_smem(const Group& g, int secondary_parts) {
+  return (size_t)(secondary_parts ? sec_smem_words(secondary_parts) : 12) * g.n * 4;
 }
 
 void launch_primary_chain(uint32_t* const* slabs_dev, int nshards, uint32_t* a_out, const Group& g,
@@ -571,7 +575,7 @@ void launch_primary_chain(uint32_t* const* slabs_dev, int nshards, uint32_t* a_o
   a.inv5 = inv5_mod2n(2 * g.n);
   a.c_first = pow_mod2n(5, g.L - 1, mask);
   a.cinv_first = pow_mod2n(a.inv5, g.L - 1, mask);
-  const size_t smem = chain_smem(g, false);
+  const size_t smem = chain_smem(g, 0);
   set_smem(primary_chain_kernel, smem);
   dim3 grid(2, SIMD * g.H, nshards);
   primary_chain_kernel<<<grid, CT, smem, st>>>(a);
@@ -592,10 +596,20 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   a.qv_stride = qv_stride;
   a.nl = nq * CTXT_PARTS;
   a.out = out;
-  const size_t smem = chain_smem(g, true);
-  set_smem(secondary_chain_kernel, smem);
-  dim3 grid(2, g.H, nq);
-  secondary_chain_kernel<<<grid, CT, smem, st>>>(a);
+  // one part per block while the chunk's blocks fit in one wave (they then
+  // share SMs with a running scan); three parts per block beyond that
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if ((long)nq * CTXT_PARTS * g.H * 2 <= sms) {
+    const size_t smem = chain_smem(g, 1);
+    set_smem(secondary_chain_kernel<1>, smem);
+    secondary_chain_kernel<1><<<dim3(2, CTXT_PARTS * g.H, nq), CT, smem, st>>>(a);
+  } else {
+    const size_t smem = chain_smem(g, CTXT_PARTS);
+    set_smem(secondary_chain_kernel<CTXT_PARTS>, smem);
+    secondary_chain_kernel<CTXT_PARTS><<<dim3(2, g.H, nq), CT, smem, st>>>(a);
+  }
 }
 
 }  // namespace dnspir

@@ -5,74 +5,54 @@
 // Queries are answered in groups of up to `batch`: one pass of the scan over
 // every shard serves the whole group (the slab is read once per group), then
 // the secondary databases are encoded and evaluated in chunks of one wave of
-// chain clusters (SMs / (2 H) queries, capped by a memory budget).  Two scan engines: CUDA cores over the lane layout (groups of 1, 2,
-// 4, 8 or 16) and the tensor cores over the tensor layout (groups up to 256,
-// tile shape per group size from a table or from dnspir_fleet_tune).
-// Two buffer slots alternate between groups: the primary phase of group k+1
-// (main stream) runs while the secondary phase of group k runs on a second,
-// high-priority stream; events order the reuse of a slot.
+// chain clusters (SMs / (2 H) queries, capped by a memory budget).  Two scan
+// engines: CUDA cores over the lane layout (groups of 1, 2, 4, 8 or 16) and
+// the tensor cores over the tensor layout (groups up to 256, tile shape per
+// group size from a table or from dnspir_fleet_tune).  Two buffer slots
+// alternate between groups: the primary phase of group k+1 (main stream) runs
+// while the secondary phase of group k runs on a second, high-priority
+// stream; events order the reuse of a slot.
 #include <algorithm>
 #include <cstring>
-#include <map>
 #include <memory>
 #include <vector>
 
-#include "host.h"
+#include "fleet_impl.h"
 
 using namespace dnspir;
 
-namespace {
-
-// Buffers of one group of queries in flight.
-struct QSlot {
-  DBuf qbytes, qnat, qbrv, fin, sec_in, reply_dev;
-  HBuf qpin;  // host staging of the query bytes
-  cudaEvent_t prim_done = nullptr, sec_done = nullptr;
-  bool sec_pending = false, prim_recorded = false;
-};
-
-}  // namespace
-
-struct dnspir_fleet {
-  int device = 0;
-  DeviceCtx* ctx = nullptr;
-  Group g1, g2;
-  uint32_t S = 0, D = 0;
-  cudaStream_t own = nullptr, st = nullptr, sec = nullptr;
-  std::vector<uint32_t*> slabs;
-  std::vector<bool> ready;
-  DBuf slabs_dev, distinct_dev, a_zq, a_ms;
-  EncodeWs ws;
-  QSlot slot[2];
-  DBuf secE, chain_out, qzq, reply_zq;  // used by one stream at a time
-  HBuf rpin;                            // host staging of the replies of one call
-  int batch = 1;
-  int sec_chunk = 1;  // queries per secondary launch sequence
-  int engine = DNSPIR_ENGINE_CUDA_CORES;
-  DBuf qb, err_word, tmp_lane;      // tensor engine: query operand, wait-error word, preprocessing scratch
-  std::map<int, int> tuned;         // tensor engine: group size -> tile shape index
-  std::vector<cudaEvent_t> tev;  // 6 timing events per group of the last call
-  std::vector<int> q_group;      // per query of the last call: its group, or -1
-  std::mutex mu;
-  ~dnspir_fleet() {
-    for (uint32_t* s : slabs)
-      if (s) cudaFree(s);
-    for (auto& e : tev)
-      if (e) cudaEventDestroy(e);
-    for (auto& s : slot) {
-      if (s.prim_done) cudaEventDestroy(s.prim_done);
-      if (s.sec_done) cudaEventDestroy(s.sec_done);
-    }
-    if (sec) cudaStreamDestroy(sec);
-    if (own) cudaStreamDestroy(own);
-  }
-};
+dnspir_fleet::~dnspir_fleet() {
+  for (uint32_t* s : slabs)
+    if (s) cudaFree(s);
+  for (auto& e : tev)
+    if (e) cudaEventDestroy(e);
+  if (sec) cudaStreamDestroy(sec);
+  if (own) cudaStreamDestroy(own);
+}
 
 namespace {
 
-const size_t QV_WORDS_PER_QUERY = 6 * 2;  // decoded slots x factors, times N
 const size_t SEC_BUDGET = (size_t)6 << 30;  // secondary workspace of one chunk
 const int TENSOR_MAX_BATCH = 256;
+
+#define NOT_SERVING(f) \
+  if ((f)->serving) return fail(DNSPIR_ERR_BAD_ARG, "the fleet is attached to a running server")
+
+int group_events(dnspir_fleet* f, uint32_t gi, cudaEvent_t** out) {
+  while (f->tev.size() < 6 * (size_t)(gi + 1)) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    f->tev.push_back(e);
+  }
+  *out = &f->tev[6 * (size_t)gi];
+  return DNSPIR_OK;
+}
+
+int pow2_batch(int nb) {
+  int b = 1;
+  while (b < nb) b <<= 1;
+  return b;
+}
 
 // Tile shape of the tensor scan for a group of nb queries, and the padded
 // group size it implies.
@@ -85,7 +65,7 @@ const TScanShape& tensor_shape(dnspir_fleet* f, int nb, int* nb_pad) {
     idx = it->second;
   } else {
     // untuned: the narrowest query tile that holds the group, one m-tile
-    const int want = nb <= 4 ? 16 : nb <= 8 ? 32 : nb <= 16 ? 64 : nb <= 32 ? 128 : 256;
+    const int want = nb <= 4 ? 16 : nb <= 8 ? 32 : nb <= 16 ? 64 : nb <= 32 ? 128 : nb <= 64 ? 256 : 512;
     idx = 0;
     for (int i = count - 1; i >= 0; i--)
       if (sh[i].nq == want && sh[i].mtpc == 1) idx = i;
@@ -95,118 +75,9 @@ const TScanShape& tensor_shape(dnspir_fleet* f, int nb, int* nb_pad) {
   return sh[idx];
 }
 
-int fleet_ready(dnspir_fleet* f) {
-  for (uint32_t d = 0; d < f->D; d++)
-    if (!f->ready[d]) return fail(DNSPIR_ERR_NOT_READY, "fleet shard not preprocessed");
-  return DNSPIR_OK;
-}
-
-int group_events(dnspir_fleet* f, uint32_t gi, cudaEvent_t** out) {
-  while (f->tev.size() < 6 * (size_t)(gi + 1)) {
-    cudaEvent_t e;
-    CK(cudaEventCreate(&e));
-    f->tev.push_back(e);
-  }
-  *out = &f->tev[6 * (size_t)gi];
-  return DNSPIR_OK;
-}
-
-int kernel_batch(int nb) {
-  int b = 1;
-  while (b < nb) b <<= 1;
-  return b;
-}
-
 int slot_acquire(dnspir_fleet* f, QSlot& s) {
   if (s.sec_pending) CK(cudaStreamWaitEvent(f->st, s.sec_done, 0));
   s.sec_pending = false;
-  return DNSPIR_OK;
-}
-
-int slot_workspace(dnspir_fleet* f, QSlot& s, int Bk, int nb) {
-  const size_t n = f->g1.n;
-  CKR(s.qnat.ensure((size_t)Bk * QV_WORDS_PER_QUERY * n * 4));
-  CKR(s.qbrv.ensure((size_t)Bk * QV_WORDS_PER_QUERY * n * 4));
-  CKR(s.fin.ensure((size_t)Bk * f->S * 2 * n * SIMD * 4));
-  CKR(s.sec_in.ensure((size_t)f->g2.l * CTXT_PARTS * nb * n * 2));
-  if (f->engine == DNSPIR_ENGINE_TENSOR) CKR(f->qb.ensure(tscan_query_bytes(f->g1, Bk)));
-  return DNSPIR_OK;
-}
-
-// Primary phase of a group on the main stream (decoded vectors already in the
-// slot): one scan pass for Bk queries, epilogue of the first nb.
-// Events: t[1] scan start, t[2] scan end, t[3] primary end.
-int stage_primary(dnspir_fleet* f, QSlot& s, int nb, int Bk, cudaEvent_t* t) {
-  const Group& g1 = f->g1;
-  const size_t n = g1.n;
-  cudaStream_t st = f->st;
-  if (Bk > nb && f->engine == DNSPIR_ENGINE_CUDA_CORES)  // unused query positions compute on zeros
-    CK(cudaMemsetAsync(s.qnat.as<uint32_t>() + (size_t)nb * QV_WORDS_PER_QUERY * n, 0,
-                       (size_t)(Bk - nb) * QV_WORDS_PER_QUERY * n * 4, st));
-  CK(cudaEventRecord(t[1], st));
-  if (f->engine == DNSPIR_ENGINE_TENSOR) {
-    int nb_pad = 0;
-    const TScanShape& shape = tensor_shape(f, nb, &nb_pad);
-    if (nb_pad != Bk) return fail(DNSPIR_ERR_BAD_ARG, "tensor scan batch mismatch");
-    if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, nb, Bk,
-                     f->qb.as<uint8_t>(), s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1,
-                     slot_maps(f->ctx, g1.log2n), shape, st))
-      return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
-  } else if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, Bk,
-                               s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), st)) {
-    return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
-  }
-  CK(cudaEventRecord(t[2], st));
-  launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
-                          s.sec_in.as<uint16_t>(), f->sec_chunk, g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, st);
-  CK(cudaEventRecord(t[3], st));
-  CK(cudaEventRecord(s.prim_done, st));
-  s.prim_recorded = true;
-  CK(cudaGetLastError());
-  return DNSPIR_OK;
-}
-
-// Secondary phase of a group on the secondary stream: encode the nb per-query
-// databases (3 lanes each), run the fused key-switch chains, write the replies
-// (bytes at reply_dev + q * reply_stride, or Z_q ciphertexts) and copy reply
-// bytes to host_reply when given.  Events: t[4] start, t[5] end.
-int stage_secondary(dnspir_fleet* f, QSlot& s, int nb, cudaEvent_t* t, uint8_t* reply_dev, size_t reply_stride,
-                    uint64_t* reply_zq, uint8_t* host_reply) {
-  const Group& g2 = f->g2;
-  const size_t n = g2.n;
-  const int cmax = std::min(nb, f->sec_chunk);
-  const int nlmax = CTXT_PARTS * cmax;
-  cudaStream_t st = f->sec;
-  // the encoder's column transforms (A) are dead before the lift writes secE:
-  // A lives at the start of secE's buffer
-  const size_t a_bytes = (size_t)g2.l * nlmax * n * 4, e_bytes = (size_t)2 * g2.H * g2.L * nlmax * n * 4;
-  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * nlmax * n * 4));
-  CKR(f->secE.ensure(std::max(a_bytes, e_bytes)));
-  CKR(f->chain_out.ensure((size_t)cmax * g2.H * CTXT_PARTS * 2 * 2 * n * 4));
-  CK(cudaStreamWaitEvent(st, s.prim_done, 0));
-  CK(cudaEventRecord(t[4], st));
-  const uint32_t l_in = f->S * SIMD;
-  const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
-  const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
-  for (int c0 = 0; c0 < nb; c0 += f->sec_chunk) {
-    const int nc = std::min(f->sec_chunk, nb - c0);
-    const int nl = CTXT_PARTS * nc;
-    const uint16_t* in = s.sec_in.as<uint16_t>() + (size_t)c0 * CTXT_PARTS * l_in * n;
-    launch_encode_cols(in, f->secE.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
-    launch_encode_rows(f->secE.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
-    launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, nl, 1, maps, f->ctx->T, st);
-    launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>() + (size_t)c0 * QV_WORDS_PER_QUERY * n,
-                           QV_WORDS_PER_QUERY * n, nc, f->chain_out.as<uint32_t>(), g2, cc, f->ctx->T, st);
-    launch_reply(f->chain_out.as<uint32_t>(), nc, g2.H, reply_dev ? reply_dev + (size_t)c0 * reply_stride : nullptr,
-                 reply_stride, reply_zq ? reply_zq + (size_t)c0 * CTXT_PARTS * 2 * n : nullptr, g2.log2n, f->ctx->T,
-                 st);
-  }
-  if (host_reply)
-    CK(cudaMemcpyAsync(host_reply, reply_dev, (size_t)nb * dnspir_reply_bytes(), cudaMemcpyDeviceToHost, st));
-  CK(cudaEventRecord(t[5], st));
-  CK(cudaEventRecord(s.sec_done, st));
-  s.sec_pending = true;
-  CK(cudaGetLastError());
   return DNSPIR_OK;
 }
 
@@ -228,7 +99,38 @@ int fleet_drain(dnspir_fleet* f) {
   return DNSPIR_OK;
 }
 
-PolySpec wire_spec(const Group& g1, const Group& g2) {
+// Scan of the decoded queries in s.qnat (kernel batch Bk) into s.fin.
+int launch_scan(dnspir_fleet* f, QSlot& s, int nb, int Bk) {
+  const Group& g1 = f->g1;
+  const size_t qv = QV_WORDS_PER_QUERY * g1.n;
+  if (f->engine == DNSPIR_ENGINE_TENSOR) {
+    int nb_pad = 0;
+    const TScanShape& shape = tensor_shape(f, nb, &nb_pad);
+    if (nb_pad != Bk) return fail(DNSPIR_ERR_BAD_ARG, "tensor scan batch mismatch");
+    if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), qv, nb, Bk, f->qb.as<uint8_t>(),
+                     s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), shape, f->st))
+      return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
+    return DNSPIR_OK;
+  }
+  if (Bk > nb)  // unused query positions of the kernel batch compute on zeros
+    CK(cudaMemsetAsync(s.qnat.as<uint32_t>() + (size_t)nb * qv, 0, (size_t)(Bk - nb) * qv * 4, f->st));
+  if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), qv, Bk, s.fin.as<uint32_t>(), g1,
+                        slot_maps(f->ctx, g1.log2n), f->st))
+    return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
+  return DNSPIR_OK;
+}
+
+}  // namespace
+
+namespace dnspir {
+
+int fleet_ready(dnspir_fleet* f) {
+  for (uint32_t d = 0; d < f->D; d++)
+    if (!f->ready[d]) return fail(DNSPIR_ERR_NOT_READY, "fleet shard not preprocessed");
+  return DNSPIR_OK;
+}
+
+PolySpec fleet_wire_spec(const dnspir_fleet* f) {
   PolySpec spec;
   memset(&spec, 0, sizeof(spec));
   uint32_t off = 0;
@@ -237,15 +139,117 @@ PolySpec wire_spec(const Group& g1, const Group& g2) {
     spec.bits[spec.npoly] = bits;
     spec.slot[spec.npoly] = slot;
     spec.npoly++;
-    off += g1.n * bits / 8;
+    off += f->g1.n * bits / 8;
   };
   add(0, GK_BITS);
   add(1, GK_BITS);
   add(2, PQ_BITS);
-  if (g1.H == 2) add(3, PQ_BITS);
+  if (f->g1.H == 2) add(3, PQ_BITS);
   add(4, SQ_BITS);
-  if (g2.H == 2) add(5, SQ_BITS);
+  if (f->g2.H == 2) add(5, SQ_BITS);
   return spec;
+}
+
+uint32_t fleet_gk_bytes(const dnspir_fleet* f) { return 2 * f->g1.n * GK_BITS / 8; }
+
+int fleet_kernel_batch(dnspir_fleet* f, int nb) {
+  int Bk = pow2_batch(nb);
+  if (f->engine == DNSPIR_ENGINE_TENSOR) tensor_shape(f, nb, &Bk);
+  return Bk;
+}
+
+int fleet_slot_workspace(dnspir_fleet* f, QSlot& s, int Bk, int nb, size_t qbytes) {
+  const size_t n = f->g1.n;
+  CKR(s.qnat.ensure((size_t)Bk * QV_WORDS_PER_QUERY * n * 4));
+  CKR(s.qbrv.ensure((size_t)Bk * QV_WORDS_PER_QUERY * n * 4));
+  CKR(s.fin.ensure((size_t)Bk * f->S * 2 * n * SIMD * 4));
+  CKR(s.sec_in.ensure((size_t)f->g2.l * CTXT_PARTS * nb * n * 2));
+  CKR(s.qdesc.ensure((size_t)nb * sizeof(QDesc)));
+  CKR(s.dpin.ensure((size_t)nb * sizeof(QDesc)));
+  if (qbytes) CKR(s.qbytes.ensure(qbytes));
+  if (f->engine == DNSPIR_ENGINE_TENSOR) CKR(f->qb.ensure(tscan_query_bytes(f->g1, Bk)));
+  return DNSPIR_OK;
+}
+
+int fleet_secondary_workspace(dnspir_fleet* f, int nb) {
+  const Group& g2 = f->g2;
+  const size_t n = g2.n;
+  const int cmax = std::min(nb, f->sec_chunk);
+  const int nlmax = CTXT_PARTS * cmax;
+  // the encoder's column transforms (A) are dead before the lift writes secE:
+  // A lives at the start of secE's buffer
+  const size_t a_bytes = (size_t)g2.l * nlmax * n * 4, e_bytes = (size_t)2 * g2.H * g2.L * nlmax * n * 4;
+  CKR(f->ws.Ahat.ensure((size_t)g2.H * g2.L * nlmax * n * 4));
+  CKR(f->secE.ensure(std::max(a_bytes, e_bytes)));
+  CKR(f->chain_out.ensure((size_t)cmax * g2.H * CTXT_PARTS * 2 * 2 * n * 4));
+  return DNSPIR_OK;
+}
+
+int fleet_primary_kernels(dnspir_fleet* f, QSlot& s, int nb, int Bk, const uint32_t* sess_nat,
+                          const uint32_t* sess_brv, cudaEvent_t scan0, cudaEvent_t scan1) {
+  const Group& g1 = f->g1;
+  const size_t qv = QV_WORDS_PER_QUERY * g1.n;
+  if (s.qbytes.p)
+    launch_decode_query(s.qbytes.as<uint8_t>(), s.qdesc.as<QDesc>(), nb, fleet_wire_spec(f), fleet_gk_bytes(f),
+                        s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), qv, sess_nat, sess_brv, g1.log2n, f->ctx->T,
+                        f->st);
+  if (scan0) CK(cudaEventRecord(scan0, f->st));
+  CKR(launch_scan(f, s, nb, Bk));
+  if (scan1) CK(cudaEventRecord(scan1, f->st));
+  launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
+                          s.sec_in.as<uint16_t>(), f->sec_chunk, g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, f->st);
+  CK(cudaGetLastError());
+  return DNSPIR_OK;
+}
+
+int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_dev, size_t reply_stride,
+                            uint64_t* reply_zq, uint8_t* host_reply) {
+  const Group& g2 = f->g2;
+  const size_t n = g2.n;
+  cudaStream_t st = f->sec;
+  const uint32_t l_in = f->S * SIMD;
+  const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
+  const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
+  for (int c0 = 0; c0 < nb; c0 += f->sec_chunk) {
+    const int nc = std::min(f->sec_chunk, nb - c0);
+    const int nl = CTXT_PARTS * nc;
+    const uint16_t* in = s.sec_in.as<uint16_t>() + (size_t)c0 * CTXT_PARTS * l_in * n;
+    launch_encode_cols(in, f->secE.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
+    launch_encode_rows(f->secE.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
+    launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, nl, 1, maps, f->ctx->T, st);
+    launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>() + (size_t)c0 * QV_WORDS_PER_QUERY * n,
+                           QV_WORDS_PER_QUERY * n, nc, f->chain_out.as<uint32_t>(), g2, cc, f->ctx->T, st);
+    launch_reply(f->chain_out.as<uint32_t>(), nc, g2.H, reply_dev ? reply_dev + (size_t)c0 * reply_stride : nullptr,
+                 reply_stride, reply_zq ? reply_zq + (size_t)c0 * CTXT_PARTS * 2 * n : nullptr, g2.log2n, f->ctx->T,
+                 st);
+  }
+  if (host_reply)
+    CK(cudaMemcpyAsync(host_reply, reply_dev, (size_t)nb * dnspir_reply_bytes(), cudaMemcpyDeviceToHost, st));
+  CK(cudaGetLastError());
+  return DNSPIR_OK;
+}
+
+}  // namespace dnspir
+
+namespace {
+
+// One group through both phases with timing events: primary on f->st,
+// secondary on f->sec after the primary.  Query bytes and descriptors (or
+// decoded vectors) must already be queued on f->st.
+int run_group(dnspir_fleet* f, QSlot& s, int nb, int Bk, cudaEvent_t* t, uint8_t* reply_dev, size_t reply_stride,
+              uint64_t* reply_zq, uint8_t* host_reply) {
+  CKR(fleet_primary_kernels(f, s, nb, Bk, nullptr, nullptr, t[1], t[2]));
+  CK(cudaEventRecord(t[3], f->st));
+  CK(cudaEventRecord(s.prim_done, f->st));
+  s.prim_recorded = true;
+  CKR(fleet_secondary_workspace(f, nb));
+  CK(cudaStreamWaitEvent(f->sec, s.prim_done, 0));
+  CK(cudaEventRecord(t[4], f->sec));
+  CKR(fleet_secondary_kernels(f, s, nb, reply_dev, reply_stride, reply_zq, host_reply));
+  CK(cudaEventRecord(t[5], f->sec));
+  CK(cudaEventRecord(s.sec_done, f->sec));
+  s.sec_pending = true;
+  return DNSPIR_OK;
 }
 
 }  // namespace
@@ -324,6 +328,7 @@ int dnspir_fleet_create(int device, uint64_t num_entries, uint32_t num_distinct,
 int dnspir_fleet_set_batch(dnspir_fleet* f, uint32_t max_batch) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   if (f->engine == DNSPIR_ENGINE_TENSOR) {
     if (max_batch < 1 || max_batch > TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
   } else if (!scan_batch_supported((int)max_batch)) {
@@ -336,6 +341,7 @@ int dnspir_fleet_set_batch(dnspir_fleet* f, uint32_t max_batch) {
 int dnspir_fleet_set_engine(dnspir_fleet* f, int engine) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   if (engine != DNSPIR_ENGINE_CUDA_CORES && engine != DNSPIR_ENGINE_TENSOR)
     return fail(DNSPIR_ERR_BAD_ARG, "unknown scan engine");
   if (engine == DNSPIR_ENGINE_TENSOR && !tensor_layout_supported(f->g1))
@@ -356,6 +362,7 @@ int dnspir_fleet_set_engine(dnspir_fleet* f, int engine) {
 int dnspir_fleet_tune(dnspir_fleet* f, uint32_t batch, double* ms_per_shape, int* chosen) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   if (f->engine != DNSPIR_ENGINE_TENSOR) return fail(DNSPIR_ERR_BAD_ARG, "tuning applies to the tensor engine");
   if (batch < 1 || batch > (uint32_t)TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
   CKR(fleet_ready(f));
@@ -428,6 +435,7 @@ int dnspir_fleet_tune(dnspir_fleet* f, uint32_t batch, double* ms_per_shape, int
 int dnspir_fleet_scan(dnspir_fleet* f, const uint32_t* qnat_dev, uint32_t nq, uint32_t* out_dev) {
   if (!f || (nq && (!qnat_dev || !out_dev))) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   CKR(fleet_ready(f));
   DeviceGuard dg(f->device);
   const Group& g1 = f->g1;
@@ -437,22 +445,10 @@ int dnspir_fleet_scan(dnspir_fleet* f, const uint32_t* qnat_dev, uint32_t nq, ui
   CKR(slot_acquire(f, s));
   for (uint32_t g0 = 0; g0 < nq; g0 += f->batch) {
     const int nb = (int)std::min<uint32_t>(f->batch, nq - g0);
-    int Bk = kernel_batch(nb);
-    if (f->engine == DNSPIR_ENGINE_TENSOR) tensor_shape(f, nb, &Bk);
-    CKR(slot_workspace(f, s, Bk, nb));
+    const int Bk = fleet_kernel_batch(f, nb);
+    CKR(fleet_slot_workspace(f, s, Bk, nb, 0));
     CK(cudaMemcpyAsync(s.qnat.p, qnat_dev + g0 * qv, (size_t)nb * qv * 4, cudaMemcpyDeviceToDevice, f->st));
-    if (Bk > nb) CK(cudaMemsetAsync(s.qnat.as<uint32_t>() + nb * qv, 0, (size_t)(Bk - nb) * qv * 4, f->st));
-    if (f->engine == DNSPIR_ENGINE_TENSOR) {
-      int pad = 0;
-      const TScanShape& shape = tensor_shape(f, nb, &pad);
-      if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), qv, nb, Bk, f->qb.as<uint8_t>(),
-                       s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), shape,
-                       f->st))
-        return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
-    } else if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), qv, Bk,
-                                 s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), f->st)) {
-      return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
-    }
+    CKR(launch_scan(f, s, nb, Bk));
     CK(cudaMemcpyAsync(out_dev + g0 * per_out, s.fin.p, (size_t)nb * per_out * 4, cudaMemcpyDeviceToDevice, f->st));
   }
   CK(cudaGetLastError());
@@ -474,6 +470,7 @@ int dnspir_fleet_set_shards(dnspir_fleet* f, uint32_t first, uint32_t count, con
                             int entries_on_device) {
   if (!f || !entries) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   if ((uint64_t)first + count > f->D) return fail(DNSPIR_ERR_BAD_ARG, "distinct shard index out of range");
   DeviceGuard dg(f->device);
   const size_t per = (size_t)SIMD * f->g1.l * f->g1.n;
@@ -521,14 +518,13 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
   const size_t RB = dnspir_reply_bytes();
   if (nq && reply_stride < RB) return fail(DNSPIR_ERR_BAD_ARG, "reply stride too small");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   CKR(fleet_ready(f));
   const Group& g1 = f->g1;
   const Group& g2 = f->g2;
   if (g1.log2n != LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_SHAPE, "the wire format is defined for N = 2048");
   DeviceGuard dg(f->device);
   const uint64_t want = dnspir_query_bytes(g1.l, g2.l);
-  const PolySpec spec = wire_spec(g1, g2);
-  const size_t qv = QV_WORDS_PER_QUERY * g1.n;
   f->q_group.assign(nq, -1);
   // validate first: rejected queries are left out of the groups
   std::vector<uint32_t> ok;
@@ -549,44 +545,45 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
   uint32_t gi = 0;
   for (size_t g0 = 0; g0 < ok.size(); g0 += f->batch, gi++) {
     const int nb = (int)std::min<size_t>(f->batch, ok.size() - g0);
-    int Bk = kernel_batch(nb);
-    if (f->engine == DNSPIR_ENGINE_TENSOR) tensor_shape(f, nb, &Bk);
+    const int Bk = fleet_kernel_batch(f, nb);
     QSlot& s = f->slot[gi & 1];
     cudaEvent_t* t = nullptr;
     CKR(group_events(f, gi, &t));
     CKR(slot_acquire(f, s));
-    CKR(slot_workspace(f, s, Bk, nb));
+    CKR(fleet_slot_workspace(f, s, Bk, nb, (size_t)nb * want));
+    // host staging of the slot may still feed the copies of the group two back
+    if (s.prim_recorded) CK(cudaEventSynchronize(s.prim_done));
+    QDesc* d = s.dpin.as<QDesc>();
+    for (int q = 0; q < nb; q++) d[q] = QDesc{(uint32_t)(q * want), -1};
     if (!on_device) {
-      CKR(s.qbytes.ensure((size_t)nb * want));
       CKR(s.qpin.ensure((size_t)nb * want));
       CKR(s.reply_dev.ensure((size_t)nb * RB));
-      // the slot's staging buffer may still feed the copy of the group two back
-      if (s.prim_recorded) CK(cudaEventSynchronize(s.prim_done));
       for (int q = 0; q < nb; q++) memcpy((uint8_t*)s.qpin.p + (size_t)q * want, queries[ok[g0 + q]], want);
     }
     CK(cudaEventRecord(t[0], f->st));
-    if (!on_device) CK(cudaMemcpyAsync(s.qbytes.p, s.qpin.p, (size_t)nb * want, cudaMemcpyHostToDevice, f->st));
-    for (int q = 0; q < nb; q++) {
-      const uint8_t* src = on_device ? queries[ok[g0 + q]] : s.qbytes.as<uint8_t>() + (size_t)q * want;
-      launch_decode_query(src, spec, s.qnat.as<uint32_t>() + q * qv, s.qbrv.as<uint32_t>() + q * qv, g1.log2n,
-                          f->ctx->T, f->st);
+    CK(cudaMemcpyAsync(s.qdesc.p, s.dpin.p, (size_t)nb * sizeof(QDesc), cudaMemcpyHostToDevice, f->st));
+    if (!on_device) {
+      CK(cudaMemcpyAsync(s.qbytes.p, s.qpin.p, (size_t)nb * want, cudaMemcpyHostToDevice, f->st));
+    } else {
+      for (int q = 0; q < nb; q++)
+        CK(cudaMemcpyAsync(s.qbytes.as<uint8_t>() + (size_t)q * want, queries[ok[g0 + q]], want,
+                           cudaMemcpyDeviceToDevice, f->st));
     }
-    CKR(stage_primary(f, s, nb, Bk, t));
     // replies of a group are contiguous in the caller's buffer only when its
     // queries are; otherwise (a rejected query inside the group) go through
     // the staging path
     bool contiguous = true;
     for (int q = 1; q < nb; q++) contiguous &= ok[g0 + q] == ok[g0] + q;
     if (on_device && contiguous) {
-      CKR(stage_secondary(f, s, nb, t, replies + (size_t)ok[g0] * reply_stride, reply_stride, nullptr, nullptr));
+      CKR(run_group(f, s, nb, Bk, t, replies + (size_t)ok[g0] * reply_stride, reply_stride, nullptr, nullptr));
     } else if (on_device) {
       CKR(s.reply_dev.ensure((size_t)nb * RB));
-      CKR(stage_secondary(f, s, nb, t, s.reply_dev.as<uint8_t>(), RB, nullptr, nullptr));
+      CKR(run_group(f, s, nb, Bk, t, s.reply_dev.as<uint8_t>(), RB, nullptr, nullptr));
       for (int q = 0; q < nb; q++)
         CK(cudaMemcpyAsync(replies + (size_t)ok[g0 + q] * reply_stride, s.reply_dev.as<uint8_t>() + q * RB, RB,
                            cudaMemcpyDeviceToDevice, f->sec));
     } else {
-      CKR(stage_secondary(f, s, nb, t, s.reply_dev.as<uint8_t>(), RB, nullptr, (uint8_t*)f->rpin.p + g0 * RB));
+      CKR(run_group(f, s, nb, Bk, t, s.reply_dev.as<uint8_t>(), RB, nullptr, (uint8_t*)f->rpin.p + g0 * RB));
     }
     for (int q = 0; q < nb; q++) f->q_group[ok[g0 + q]] = (int)gi;
   }
@@ -611,6 +608,7 @@ int dnspir_fleet_perform_double_pir(dnspir_fleet* f, const uint64_t* pq, const u
                                     const uint64_t* sqc, const uint64_t* gk, uint64_t* out) {
   if (!f || !pq || !sq || !gk || !out) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   CKR(fleet_ready(f));
   if ((f->g1.H == 2) != (pqc != nullptr))
     return fail(DNSPIR_ERR_BAD_SHAPE, "conjugate primary query must be given exactly when required (double_pir.rs:160)");
@@ -626,20 +624,25 @@ int dnspir_fleet_perform_double_pir(dnspir_fleet* f, const uint64_t* pq, const u
   if (sqc) memcpy(&z[5 * n], sqc, n * 8);
   if (!reduced(z.data(), z.size())) return fail(DNSPIR_ERR_BAD_ARG, "ring element coefficients must be below q");
   DeviceGuard dg(f->device);
-  QSlot& s = f->slot[0];
+  // a private slot without query bytes: the ring elements go straight to the
+  // decoded vectors
+  QSlot s;
+  CK(cudaEventCreateWithFlags(&s.prim_done, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s.sec_done, cudaEventDisableTiming));
+  for (auto& o : f->slot) CKR(slot_acquire(f, o));
+  const int Bk = fleet_kernel_batch(f, 1);
   cudaEvent_t* t = nullptr;
   CKR(group_events(f, 0, &t));
-  CKR(slot_acquire(f, s));
-  CKR(slot_workspace(f, s, 1, 1));
+  CKR(fleet_slot_workspace(f, s, Bk, 1, 0));
   CKR(f->qzq.ensure(z.size() * 8));
   CKR(f->reply_zq.ensure((size_t)CTXT_PARTS * 2 * n * 8));
   CK(cudaEventRecord(t[0], f->st));
   CK(cudaMemcpyAsync(f->qzq.p, z.data(), z.size() * 8, cudaMemcpyHostToDevice, f->st));
   launch_ring_to_ntt(f->qzq.as<uint64_t>(), 6, s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), f->g1.log2n, f->ctx->T,
                      f->st);
-  CKR(stage_primary(f, s, 1, 1, t));
-  CKR(stage_secondary(f, s, 1, t, nullptr, 0, f->reply_zq.as<uint64_t>(), nullptr));
+  CKR(run_group(f, s, 1, Bk, t, nullptr, 0, f->reply_zq.as<uint64_t>(), nullptr));
   f->q_group.assign(1, 0);
+  CK(cudaStreamWaitEvent(f->st, s.sec_done, 0));
   CKR(fleet_drain(f));
   CK(cudaMemcpy(out, f->reply_zq.p, (size_t)CTXT_PARTS * 2 * n * 8, cudaMemcpyDeviceToHost));
   return DNSPIR_OK;
@@ -694,6 +697,7 @@ int dnspir_fleet_last_timings(dnspir_fleet* f, double* primary_ms, double* secon
 int dnspir_fleet_set_stream(dnspir_fleet* f, void* s) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
   std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
   f->st = s ? (cudaStream_t)s : f->own;
   return DNSPIR_OK;
 }
@@ -702,6 +706,7 @@ uint64_t dnspir_fleet_slab_bytes(dnspir_fleet* f) { return f ? (uint64_t)f->D * 
 
 int dnspir_fleet_destroy(dnspir_fleet* f) {
   if (!f) return DNSPIR_OK;
+  if (f->serving) return fail(DNSPIR_ERR_BAD_ARG, "the fleet is attached to a running server");
   DeviceGuard dg(f->device);
   cudaStreamSynchronize(f->st);
   cudaStreamSynchronize(f->sec);

@@ -83,6 +83,10 @@ struct HBuf {
     bytes = b;
     return DNSPIR_OK;
   }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
 };
 
 // -------------------------------------------------------------- shard state

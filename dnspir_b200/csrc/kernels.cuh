@@ -129,8 +129,17 @@ struct PolySpec {
   int slot[6];       // destination slot: 0 gk0, 1 gk1, 2 pq, 3 pqc, 4 sq, 5 sqc
   int npoly;
 };
-void launch_decode_query(const uint8_t* bytes, const PolySpec& spec, uint32_t* qnat, uint32_t* qbrv, int log2n,
-                         const NttTables& T, cudaStream_t st);
+// Per query of a group: offset of its bytes, and its session slot (-1: the
+// query carries its own Galois keys; otherwise they come from the session
+// cache and the bytes omit them, gk_bytes shorter).
+struct QDesc {
+  uint32_t byte_off;
+  int32_t session;
+};
+// nq queries, outputs at q * q_stride words.
+void launch_decode_query(const uint8_t* bytes, const QDesc* desc, int nq, const PolySpec& spec, uint32_t gk_bytes,
+                         uint32_t* qnat, uint32_t* qbrv, size_t q_stride, const uint32_t* sess_nat,
+                         const uint32_t* sess_brv, int log2n, const NttTables& T, cudaStream_t st);
 // Ring elements (Z_q, u64) -> NTT vectors, natural [i][p][u] and bit-reversed [i][p][pos].
 void launch_ring_to_ntt(const uint64_t* zq, int count, uint32_t* qnat, uint32_t* qbrv, int log2n, const NttTables& T,
                         cudaStream_t st);

@@ -405,7 +405,7 @@ const TScanShape* tscan_shapes(int* count) {
   // CTAs per SM
   static const TScanShape shapes[] = {
       {16, 1, 5},  {16, 1, 10}, {32, 1, 5},  {64, 1, 4},  {64, 2, 3},  {128, 1, 3},
-      {128, 2, 3}, {256, 1, 3}, {256, 1, 4}, {256, 2, 2}, {256, 2, 3},
+      {128, 2, 3}, {256, 1, 3}, {256, 1, 4}, {256, 2, 2}, {256, 2, 3}, {512, 1, 2},
   };
   *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
   return shapes;
@@ -451,6 +451,7 @@ int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, s
     case 1282: return launch_t<128, 2>(a, stg, st);
     case 2561: return launch_t<256, 1>(a, stg, st);
     case 2562: return launch_t<256, 2>(a, stg, st);
+    case 5121: return launch_t<512, 1>(a, stg, st);
     default: return -1;
   }
 }

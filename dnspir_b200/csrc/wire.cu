@@ -33,23 +33,39 @@ __device__ __forceinline__ uint64_t unpack_one(const uint8_t* __restrict__ b, in
   return x;
 }
 
-// grid: x = polynomial of the query, y = factor.  Outputs natural-order
-// qnat[slot][p][u] and bit-reversed qbrv[slot][p][pos].
-__global__ void decode_query_kernel(const uint8_t* __restrict__ bytes, PolySpec spec, uint32_t* __restrict__ qnat,
-                                    uint32_t* __restrict__ qbrv, int log2n, NttTables T) {
+// grid: x = polynomial of the query, y = factor, z = query of the group.
+// Outputs natural-order qnat[slot][p][u] and bit-reversed qbrv[slot][p][pos]
+// at q * q_stride.  A query with a session takes its Galois-key slots 0 and 1
+// from the session cache ([session][slot][p][N], natural and bit-reversed)
+// and its bytes start with the first polynomial after the keys.
+__global__ void decode_query_kernel(const uint8_t* __restrict__ bytes, const QDesc* __restrict__ desc, PolySpec spec,
+                                    uint32_t gk_bytes, uint32_t* __restrict__ qnat, uint32_t* __restrict__ qbrv,
+                                    size_t q_stride, const uint32_t* __restrict__ sess_nat,
+                                    const uint32_t* __restrict__ sess_brv, int log2n, NttTables T) {
   extern __shared__ uint32_t sm[];
-  const int poly = blockIdx.x, p = blockIdx.y;
+  const int poly = blockIdx.x, p = blockIdx.y, q = blockIdx.z;
   const uint32_t N = 1u << log2n;
   const uint32_t pr = prime_of(p);
   const int bits = spec.bits[poly];
-  const uint8_t* src = bytes + spec.off[poly];
+  const QDesc d = desc[q];
+  const int slot = spec.slot[poly];
+  qnat += (size_t)q * q_stride;
+  qbrv += (size_t)q * q_stride;
+  if (d.session >= 0 && slot < 2) {
+    const size_t o = (((size_t)d.session * 2 + slot) * 2 + p) * N;
+    for (uint32_t u = threadIdx.x; u < N; u += blockDim.x) {
+      qnat[((size_t)slot * 2 + p) * N + u] = sess_nat[o + u];
+      qbrv[((size_t)slot * 2 + p) * N + u] = sess_brv[o + u];
+    }
+    return;
+  }
+  const uint8_t* src = bytes + d.byte_off + spec.off[poly] - (d.session >= 0 ? gk_bytes : 0);
   for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
     const uint64_t v = ms_decode(unpack_one(src, bits, N, n), bits);
     sm[n] = reduce64(v, pr, barrett_mu(pr));
   }
   __syncthreads();
   ntt_fwd_smem(sm, log2n, 1, T, p);
-  const int slot = spec.slot[poly];
   uint32_t* on = qnat + ((size_t)slot * 2 + p) * N;
   uint32_t* ob = qbrv + ((size_t)slot * 2 + p) * N;
   for (uint32_t u = threadIdx.x; u < N; u += blockDim.x) {
@@ -130,10 +146,13 @@ __global__ void reply_kernel(const uint32_t* __restrict__ chain_out, int H, uint
 
 CrtConst host_crt_const();
 
-void launch_decode_query(const uint8_t* bytes, const PolySpec& spec, uint32_t* qnat, uint32_t* qbrv, int log2n,
-                         const NttTables& T, cudaStream_t st) {
-  dim3 grid(spec.npoly, 2);
-  decode_query_kernel<<<grid, 256, (size_t)4 << log2n, st>>>(bytes, spec, qnat, qbrv, log2n, T);
+void launch_decode_query(const uint8_t* bytes, const QDesc* desc, int nq, const PolySpec& spec, uint32_t gk_bytes,
+                         uint32_t* qnat, uint32_t* qbrv, size_t q_stride, const uint32_t* sess_nat,
+                         const uint32_t* sess_brv, int log2n, const NttTables& T, cudaStream_t st) {
+  if (nq <= 0) return;
+  dim3 grid(spec.npoly, 2, nq);
+  decode_query_kernel<<<grid, 256, (size_t)4 << log2n, st>>>(bytes, desc, spec, gk_bytes, qnat, qbrv, q_stride,
+                                                              sess_nat, sess_brv, log2n, T);
 }
 
 void launch_ring_to_ntt(const uint64_t* zq, int count, uint32_t* qnat, uint32_t* qbrv, int log2n, const NttTables& T,

@@ -141,6 +141,45 @@ int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, ui
 /* The tensor scan's tile shapes (query-operand rows per CTA, m-tiles per CTA,
  * pipeline stages); returns their count. */
 int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int max);
+
+/* ---- Serving loop (no counterpart in the reference, whose server answers each
+ * connection on its own thread with process_query, dns/server.rs:789).
+ * One worker thread per server owns the device work of every database added
+ * to it: submitted queries are queued per database and answered in groups
+ * (continuous batching: each group takes every pending query up to the
+ * database's admitted group size, while earlier groups are still on the
+ * device); each group size's launch sequence is captured as CUDA graphs and
+ * replayed.  Group sizes are admitted by free device memory at start.  A fleet
+ * attached to a running server answers only through it (its other calls
+ * return DNSPIR_ERR_BAD_ARG until dnspir_server_stop).
+ * Sessions: a client's Galois keys (the first two polynomials of its query
+ * bytes, 25,600 bytes) decoded once and held on the device; a query submitted
+ * with a session omits those bytes.  max_sessions may be 0. */
+typedef struct dnspir_server dnspir_server;
+int dnspir_server_create(int device, uint32_t max_sessions, dnspir_server** out);
+/* max_batch: 1..256 (tensor engine) or 1, 2, 4, 8, 16 (CUDA cores). */
+int dnspir_server_add_db(dnspir_server* server, dnspir_fleet* fleet, uint32_t max_batch, uint32_t* db_id);
+int dnspir_server_start(dnspir_server* server, int use_graphs);
+int dnspir_server_open_session(dnspir_server* server, const uint8_t* galois_key_bytes, uint64_t len,
+                               uint64_t* session);
+/* Requests already submitted with the session still complete. */
+int dnspir_server_close_session(dnspir_server* server, uint64_t session);
+/* session: -1 for a full query (the reference's bytes). */
+int dnspir_server_submit(dnspir_server* server, uint32_t db_id, int64_t session, const uint8_t* query, uint64_t len,
+                         uint64_t* ticket);
+/* *done = 0 while pending; once done the reply (22,272 bytes) is copied out,
+ * the ticket is released and the request's status is returned. */
+int dnspir_server_poll(dnspir_server* server, uint64_t ticket, uint8_t* reply, uint64_t reply_cap, int* done);
+int dnspir_server_wait(dnspir_server* server, uint64_t ticket, uint8_t* reply, uint64_t reply_cap,
+                       uint32_t timeout_ms);
+/* Completed requests, admitted group size, groups launched (and of them,
+ * replayed from graphs), and the submit-to-done latencies in completion order. */
+int dnspir_server_db_stats(dnspir_server* server, uint32_t db_id, uint64_t* completed, uint32_t* admitted_batch,
+                           uint64_t* groups, uint64_t* graph_groups, double* latencies_ms, uint32_t max_latencies,
+                           uint32_t* n_latencies);
+/* Answers every submitted request, then detaches the fleets. */
+int dnspir_server_stop(dnspir_server* server);
+int dnspir_server_destroy(dnspir_server* server);
 /* Synthetic 2560-byte payloads packed into 10-bit coefficients
  * (pack_bytes_into_coeffs, dns/bucket.rs:289-303): bytes = entries x 2560 on
  * the device, coeffs = entries x 2048 on the device. */
