@@ -21,6 +21,14 @@ responses/s, p50/p99 per-query latency and the scan's effective GB/s
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                   [--engine tensor|cuda] [--batched 16,64,128]
+  python bench.py --serve [--serve-rate 5000] [--serve-seconds 10]
+
+--serve measures the served mix instead: four resident databases (2^15,
+2^18, 2^20 and 2^22 entries; the last on as many distinct shards as fit),
+open-loop Poisson arrivals at the given total rate split by --serve-mix,
+answered by the serving loop (continuous batching, CUDA graphs, half of the
+clients on device-resident sessions).  One JSON line: responses/s delivered
+and p50/p99 submit-to-reply latency per database.
 
 --gpus N > 1 runs under torchrun: every rank holds a replica of the database
 and answers its own queries (queries are the units; no data-path collective),
@@ -68,6 +76,11 @@ def parse():
     ap.add_argument("--batched", default="16,64,128", help="comma-separated group sizes measured after the plain run")
     ap.add_argument("--batched-groups", type=int, default=3, help="timed groups per batched size")
     ap.add_argument("--reserve-gib", type=float, default=22.0, help="HBM left free for workspaces")
+    ap.add_argument("--serve", action="store_true", help="served mix over four databases instead")
+    ap.add_argument("--serve-rate", default="5000", help="offered queries/s (comma-separated for several runs)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-mix", default="0.7,0.2,0.08,0.02", help="shares of 2^15, 2^18, 2^20, 2^22")
+    ap.add_argument("--serve-clients", type=int, default=64, help="distinct clients per database")
     return ap.parse_args()
 
 
@@ -156,6 +169,128 @@ def shard_payload(torch, d, entries_per_shard, device, seed0=1000):
     return torch.randint(0, 256, (entries_per_shard, PAYLOAD), dtype=torch.uint8, device=device, generator=g)
 
 
+def run_serve(args, rank, local_rank):
+    """Served mix (continuous batching over four resident databases)."""
+    import torch
+    import dnspir_b200 as dp
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sizes = [1 << 15, 1 << 18, 1 << 20, 1 << 22]
+    shares = [float(x) for x in args.serve_mix.split(",")]
+    batch_cap = {1 << 15: 256, 1 << 18: 256, 1 << 20: 128, 1 << 22: 64}
+    fleets, shapes, distinct = [], [], []
+    t0 = time.time()
+    for e in sizes:
+        l1, l2, shards = dp.get_database_shape(e)
+        slab = dp.required_memory_general(11, l1) * 32
+        free, _ = torch.cuda.mem_get_info()
+        d = shards if e < (1 << 22) else max(1, min(shards, int((free - (40 << 30)) // slab)))
+        f = dp.Fleet(e, d, device=local_rank)
+        f.set_engine(dp.ENGINE_TENSOR)
+        for first in range(0, d, 8):
+            cnt = min(8, d - first)
+            co = torch.empty((cnt, 8 * l1, dp.N), dtype=torch.uint16, device=dev)
+            for i in range(cnt):
+                dp.pack_payloads(shard_payload(torch, first + i, 8 * l1, dev, seed0=7000 + 100 * sizes.index(e)),
+                                 co[i], device=local_rank)
+            f.set_shards(first, co)
+            del co
+        fleets.append(f)
+        shapes.append((l1, l2, shards))
+        distinct.append(d)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    prep_s = time.time() - t0
+    # client pools: full queries, and for half of the clients a session (keys sent once)
+    gk = dp.GALOIS_KEY_BYTES
+    pools = []
+    for di, (l1, l2, shards) in enumerate(shapes):
+        rng = np.random.default_rng(100 + di)
+        pool = []
+        for c in range(args.serve_clients):
+            i, j = int(rng.integers(0, 8 * l1)), int(rng.integers(0, shards))
+            q, sk = dp.prepare_query(hashlib.sha256(f"serve-{di}-{c}".encode()).digest(), i, j, l1, l2)
+            pool.append((q, sk, i, j))
+        pools.append(pool)
+    results = []
+    for rate in [float(r) for r in args.serve_rate.split(",")]:
+        sv = dp.Server(max_sessions=2 * args.serve_clients * len(sizes), device=local_rank)
+        ids = [sv.add_db(f, batch_cap[e]) for f, e in zip(fleets, sizes)]
+        sv.start(graphs=True)
+        sessions = [[sv.open_session(q[:gk]) if c % 2 else -1 for c, (q, _, _, _) in enumerate(pool)]
+                    for pool in pools]
+        # warm-up: one query per database and group size 1 (captures graphs)
+        for di in range(len(sizes)):
+            sv.wait(sv.submit(ids[di], pools[di][0][0]))
+        arrivals = np.random.default_rng(7)
+        n_total = int(rate * args.serve_seconds)
+        gaps = arrivals.exponential(1.0 / rate, size=n_total)
+        which = arrivals.choice(len(sizes), size=n_total, p=np.array(shares) / sum(shares))
+        clients = arrivals.integers(0, args.serve_clients, size=n_total)
+        tickets = []
+        t_start = time.perf_counter()
+        t_next = t_start
+        for k in range(n_total):
+            t_next += gaps[k]
+            while True:
+                dt = t_next - time.perf_counter()
+                if dt <= 0:
+                    break
+                if dt > 2e-4:
+                    time.sleep(dt - 1e-4)
+            di, c = int(which[k]), int(clients[k])
+            q = pools[di][c][0]
+            s = sessions[di][c]
+            tickets.append((di, c, sv.submit(ids[di], q[gk:] if s >= 0 else q, session=s)))
+        t_submitted = time.perf_counter()
+        ok, bad = 0, 0
+        checked = set()
+        for di, c, t in tickets:
+            r = sv.wait(t, timeout_ms=600000)
+            if (di, c) not in checked and len(checked) < 32:
+                checked.add((di, c))
+                q, sk, i, j = pools[di][c]
+                want = pack_host(shard_payload(torch, j % distinct[di], 8 * shapes[di][0], dev,
+                                               seed0=7000 + 100 * di)[i].cpu().numpy().tobytes())
+                if np.array_equal(dp.process_reply(r, sk), want):
+                    ok += 1
+                else:
+                    bad += 1
+        t_end = time.perf_counter()
+        per_db = {}
+        for di, e in enumerate(sizes):
+            st = sv.stats(ids[di])
+            lat = st["latencies_ms"][1:]  # drop the warm-up query
+            per_db[f"2^{e.bit_length() - 1}"] = {
+                "offered_per_sec": rate * shares[di] / sum(shares), "completed": int(len(lat)),
+                "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+                "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+                "admitted_batch": st["admitted_batch"], "groups": st["groups"] - 1,
+                "graph_groups": st["graph_groups"], "distinct_shards": distinct[di], "shards": shapes[di][2]}
+        sv.stop()
+        sv.close()
+        if bad:
+            print(json.dumps({"error": f"served mix: {bad} of {ok + bad} sampled replies failed decryption"}))
+            return 1
+        results.append({"offered_per_sec": rate, "responses_per_sec": n_total / (t_end - t_start),
+                        "submit_seconds": t_submitted - t_start, "drain_seconds": t_end - t_submitted,
+                        "per_db": per_db, "checked": {"decrypted_ok": ok, "of": ok + bad}})
+    line = {"metric": "served_mix_responses_per_sec", "value": results[0]["responses_per_sec"],
+            "unit": "responses/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "served mix: Poisson arrivals over four resident databases (2^15, 2^18, 2^20, "
+                                   "2^22 entries x 2560 B), continuous batching, CUDA graphs, half of the clients "
+                                   "on device-resident sessions", "mix": shares, "clients_per_db": args.serve_clients,
+                                   "seconds": args.serve_seconds, "engine": "tensor"},
+            "runs": results, "preprocess_s": prep_s,
+            "latency_note": "submit-to-reply wall time on the host, queueing included"}
+    print(json.dumps(line), flush=True)
+    for f in fleets:
+        f.close()
+    return 0
+
+
 def run_reference(args, rank):
     """CPU restatement of the reference's answer path, timed on the host cores."""
     if rank != 0:
@@ -213,6 +348,8 @@ def main():
     rank, local_rank, world = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.serve:
+        return run_serve(args, rank, local_rank)
 
     import torch
     import dnspir_b200 as dp
@@ -352,11 +489,11 @@ def main():
                 shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
                          "tuned_ms": round(float(tms[ch]), 3)}
             fleet.set_batch(B)
-            nq = B * args.batched_groups
+            nq = B * max(2, args.batched_groups)
             sel = torch.arange(nq, device=dev) % pool_n
             qin = pdev[sel].contiguous()
             rout = torch.zeros((nq, dp.reply_bytes()), dtype=torch.uint8, device=dev)
-            fleet.process_queries_device(qin[:B], rout[:B])  # warm-up group
+            fleet.process_queries_device(qin[:2 * B], rout[:2 * B])  # warm-up: both buffer slots
             barrier()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
