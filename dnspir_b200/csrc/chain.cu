@@ -87,11 +87,15 @@ __device__ __forceinline__ void gs_bf(uint32_t& x, uint32_t& y, uint32_t w, uint
 // LN vectors `stride` words apart, transformed together: one barrier per pass,
 // and each thread handles the same butterfly group of every vector with its
 // loads issued before the arithmetic (twiddles loaded once).
-template <int LN>
-__device__ __forceinline__ void fwd_multi(uint32_t* x0, int stride, int logn, const uint32_t* __restrict__ tw,
+// LOGN > 0 fixes the length at compile time (the stage loop unrolls and every
+// index shift is a constant); LOGN = 0 takes logn_rt.
+template <int LN, int LOGN>
+__device__ __forceinline__ void fwd_multi(uint32_t* x0, int stride, int logn_rt, const uint32_t* __restrict__ tw,
                                           const uint32_t* __restrict__ twq, uint32_t p) {
+  const int logn = LOGN ? LOGN : logn_rt;
   const int N = 1 << logn;
   int s = 0;
+#pragma unroll
   for (; s + 1 < logn; s += 2) {
     const int logt2 = logn - s - 2;
     const int t2 = 1 << logt2, t = 2 * t2, m = 1 << s;
@@ -143,11 +147,13 @@ __device__ __forceinline__ void fwd_multi(uint32_t* x0, int stride, int logn, co
   __syncthreads();
 }
 
-template <int LN>
-__device__ __forceinline__ void inv_multi(uint32_t* x0, int stride, int logn, const uint32_t* __restrict__ tw,
+template <int LN, int LOGN>
+__device__ __forceinline__ void inv_multi(uint32_t* x0, int stride, int logn_rt, const uint32_t* __restrict__ tw,
                                           const uint32_t* __restrict__ twq, uint32_t p) {
+  const int logn = LOGN ? LOGN : logn_rt;
   const int N = 1 << logn;
   int s = 0;
+#pragma unroll
   for (; s + 1 < logn; s += 2) {
     const int t = 1 << s;
     const int h0 = N >> (s + 1), h1 = N >> (s + 2);
@@ -234,10 +240,11 @@ struct ChainArgs {
 //   X[2]               2N        iNTT outputs published to the peer block
 //   CG0, CG1, CQA      3N        gk_a0 R, gk_a1 R, qry_a R of this factor and half
 //   FW, FWQ, IW, IWQ   4N        twiddles of this factor
+template <int LOGN>
 __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane, int s, uint32_t* sm) {
   cg::cluster_group cluster = cg::this_cluster();
   const int p = (int)cluster.block_rank();
-  const int logn = a.g.log2n;
+  const int logn = LOGN ? LOGN : a.g.log2n;
   const int N = 1 << logn;
   const uint32_t mask = 2 * N - 1;
   const ChainPrime cp = a.cp[p];
@@ -300,7 +307,7 @@ __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane
       }
     }
     __syncthreads();
-    inv_multi<1>(D, 0, logn, IW, IWQ, pr);
+    inv_multi<1, LOGN>(D, 0, logn, IW, IWQ, pr);
     uint32_t* Xc = X + (i & 1) * N;
     for (int b = threadIdx.x; b < N; b += CT) Xc[b] = D[b];
     cluster.sync();
@@ -311,7 +318,7 @@ __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane
       D[b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
     }
     __syncthreads();
-    fwd_multi<1>(D, 0, logn, FW, FWQ, pr);
+    fwd_multi<1, LOGN>(D, 0, logn, FW, FWQ, pr);
 #pragma unroll
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
@@ -345,29 +352,25 @@ __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane
 // part0 + LN - 1.  With LN = 3 each transform pass and cluster barrier serves
 // three vectors (throughput: one wave holds SMs / (2 H) queries); with LN = 1
 // the block needs 128 KiB and shares an SM with a scan block (latency: the
-// chains of a few queries overlap the next scan).  Shared memory (u32 words):
-//   CG0 CG1 CQA QG0 QG1 QQB   6N   gk_a0, gk_a1, qry_a, gk_b0, gk_b1, qry_b (Montgomery form)
+// chains of a few queries overlap the next scan).  The key constants gk_a0,
+// gk_a1, qry_a, gk_b0, gk_b1, qry_b (Montgomery form) and the sigma_5
+// destinations of a thread's positions live in its registers.  Shared memory
+// (u32 words):
 //   FW FWQ IW IWQ             4N   twiddles of this factor
 //   per part: A TC D X0 X1 B  6N   a, saved sigma_5(a), work vector, published iNTT x2, b
-// (10 + 6 LN) N words: 224 KiB for LN = 3, 128 KiB for LN = 1 at N = 2048.
+// (4 + 6 LN) N words: 176 KiB for LN = 3, 80 KiB for LN = 1 at N = 2048.
 constexpr int SEC_PART_WORDS = 6;  // x N
-__host__ __device__ constexpr int sec_smem_words(int ln) { return 10 + ln * SEC_PART_WORDS; }
+__host__ __device__ constexpr int sec_smem_words(int ln) { return 4 + ln * SEC_PART_WORDS; }
 
-template <int LN>
+template <int LN, int LOGN>
 __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q, int part0, uint32_t* sm) {
   cg::cluster_group cluster = cg::this_cluster();
   const int p = (int)cluster.block_rank();
-  const int logn = a.g.log2n;
+  const int logn = LOGN ? LOGN : a.g.log2n;
   const int N = 1 << logn;
   const ChainPrime cp = a.cp[p];
   const uint32_t pr = cp.p;
-  uint32_t* CG0 = sm;
-  uint32_t* CG1 = CG0 + N;
-  uint32_t* CQA = CG1 + N;
-  uint32_t* QG0 = CQA + N;
-  uint32_t* QG1 = QG0 + N;
-  uint32_t* QQB = QG1 + N;
-  uint32_t* FW = QQB + N;
+  uint32_t* FW = sm;
   uint32_t* FWQ = FW + N;
   uint32_t* IW = FWQ + N;
   uint32_t* IWQ = IW + N;
@@ -375,14 +378,23 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
   const int PS = SEC_PART_WORDS * N;
   const int oTC = N, oD = 2 * N, oX = 3 * N, oB = 5 * N;
   const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
+  constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
+  uint32_t kc[6][PER], dst[PER];
+#pragma unroll
+  for (int c = 0; c < PER; c++) {
+    const int pos = threadIdx.x + c * CT;
+    if (pos < N) {
+      const size_t o = (size_t)p * N + pos;
+      kc[0][c] = mont_reduce((uint64_t)a.gka[o] * cp.r2, pr, cp.pinv);
+      kc[1][c] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
+      kc[2][c] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, pr, cp.pinv);
+      kc[3][c] = mont_reduce((uint64_t)qq[o] * cp.r2, pr, cp.pinv);
+      kc[4][c] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
+      kc[5][c] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, pr, cp.pinv);
+      dst[c] = __ldg(a.galb + pos);
+    }
+  }
   for (int b = threadIdx.x; b < N; b += CT) {
-    const size_t o = (size_t)p * N + b;
-    CG0[b] = mont_reduce((uint64_t)a.gka[o] * cp.r2, pr, cp.pinv);
-    CG1[b] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
-    CQA[b] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, pr, cp.pinv);
-    QG0[b] = mont_reduce((uint64_t)qq[o] * cp.r2, pr, cp.pinv);
-    QG1[b] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, pr, cp.pinv);
-    QQB[b] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, pr, cp.pinv);
     FW[b] = a.T.fw[p][b];
     FWQ[b] = a.T.fwq[p][b];
     IW[b] = a.T.iw[p][b];
@@ -395,7 +407,6 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
   }
   cluster.sync();
   const uint32_t* peer = cluster.map_shared_rank(P0, p ^ 1);
-  constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
   for (uint32_t i = 0; i < a.g.L; i++) {
     // entries of row i (the three parts' lanes are adjacent), consumed at the end of the step
     const uint32_t* Ei = a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + (size_t)q * CTXT_PARTS + part0) * N;
@@ -417,17 +428,16 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
       if (pos < N) {
-        const uint32_t dst = __ldg(a.galb + pos);
 #pragma unroll
         for (int t = 0; t < LN; t++) {
-          P0[t * PS + oTC + dst] = ra[t][c];
-          P0[t * PS + oD + dst] = ra[t][c];
-          P0[t * PS + oB + dst] = rb[t][c];
+          P0[t * PS + oTC + dst[c]] = ra[t][c];
+          P0[t * PS + oD + dst[c]] = ra[t][c];
+          P0[t * PS + oB + dst[c]] = rb[t][c];
         }
       }
     }
     __syncthreads();
-    inv_multi<LN>(P0 + oD, PS, logn, IW, IWQ, pr);
+    inv_multi<LN, LOGN>(P0 + oD, PS, logn, IW, IWQ, pr);
     const int xo = oX + (int)(i & 1) * N;
     for (int b = threadIdx.x; b < N; b += CT)
 #pragma unroll
@@ -445,13 +455,13 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
       }
     }
     __syncthreads();
-    fwd_multi<LN>(P0 + oD, PS, logn, FW, FWQ, pr);
+    fwd_multi<LN, LOGN>(P0 + oD, PS, logn, FW, FWQ, pr);
 #pragma unroll
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
       if (pos < N) {
-        const uint32_t cg0 = CG0[pos], cg1 = CG1[pos], cqa = CQA[pos];
-        const uint32_t qg0 = QG0[pos], qg1 = QG1[pos], qqb = QQB[pos];
+        const uint32_t cg0 = kc[0][c], cg1 = kc[1][c], cqa = kc[2][c];
+        const uint32_t qg0 = kc[3][c], qg1 = kc[4][c], qqb = kc[5][c];
 #pragma unroll
         for (int t = 0; t < LN; t++) {
           uint32_t* P = P0 + t * PS;
@@ -476,17 +486,18 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
 }
 
 // grid: x = factor (cluster of 2), y = (part group) * H + half, z = query
-template <int LN>
+template <int LN, int LOGN>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT) secondary_chain_kernel(ChainArgs a) {
   extern __shared__ uint32_t sm[];
-  secondary_body<LN>(a, blockIdx.y % a.g.H, blockIdx.z, (blockIdx.y / a.g.H) * LN, sm);
+  secondary_body<LN, LOGN>(a, blockIdx.y % a.g.H, blockIdx.z, (blockIdx.y / a.g.H) * LN, sm);
 }
 
 // grid: x = factor (cluster of 2), y = lane * H + half, z = shard
+template <int LOGN>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT) primary_chain_kernel(ChainArgs a) {
   extern __shared__ uint32_t sm[];
   const int h = blockIdx.y % a.g.H, lane = blockIdx.y / a.g.H;
-  primary_body(a, h, lane, blockIdx.z, sm);
+  primary_body<LOGN>(a, h, lane, blockIdx.z, sm);
 }
 
 // reply_a = a_main + a_conj -> iNTT -> CRT; also the 17-bit mod switch
@@ -576,9 +587,14 @@ void launch_primary_chain(uint32_t* const* slabs_dev, int nshards, uint32_t* a_o
   a.c_first = pow_mod2n(5, g.L - 1, mask);
   a.cinv_first = pow_mod2n(a.inv5, g.L - 1, mask);
   const size_t smem = chain_smem(g, 0);
-  set_smem(primary_chain_kernel, smem);
   dim3 grid(2, SIMD * g.H, nshards);
-  primary_chain_kernel<<<grid, CT, smem, st>>>(a);
+  if (g.log2n == LOG2_N_MAX) {
+    set_smem(primary_chain_kernel<LOG2_N_MAX>, smem);
+    primary_chain_kernel<LOG2_N_MAX><<<grid, CT, smem, st>>>(a);
+  } else {
+    set_smem(primary_chain_kernel<0>, smem);
+    primary_chain_kernel<0><<<grid, CT, smem, st>>>(a);
+  }
 }
 
 void launch_primary_finalize(const uint32_t* a_out, int nshards, uint64_t* a_zq, uint32_t* a_ms, const Group& g,
@@ -601,14 +617,27 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   int sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool full = g.log2n == LOG2_N_MAX;
   if ((long)nq * CTXT_PARTS * g.H * 2 <= sms) {
     const size_t smem = chain_smem(g, 1);
-    set_smem(secondary_chain_kernel<1>, smem);
-    secondary_chain_kernel<1><<<dim3(2, CTXT_PARTS * g.H, nq), CT, smem, st>>>(a);
+    const dim3 grid(2, CTXT_PARTS * g.H, nq);
+    if (full) {
+      set_smem(secondary_chain_kernel<1, LOG2_N_MAX>, smem);
+      secondary_chain_kernel<1, LOG2_N_MAX><<<grid, CT, smem, st>>>(a);
+    } else {
+      set_smem(secondary_chain_kernel<1, 0>, smem);
+      secondary_chain_kernel<1, 0><<<grid, CT, smem, st>>>(a);
+    }
   } else {
     const size_t smem = chain_smem(g, CTXT_PARTS);
-    set_smem(secondary_chain_kernel<CTXT_PARTS>, smem);
-    secondary_chain_kernel<CTXT_PARTS><<<dim3(2, g.H, nq), CT, smem, st>>>(a);
+    const dim3 grid(2, g.H, nq);
+    if (full) {
+      set_smem(secondary_chain_kernel<CTXT_PARTS, LOG2_N_MAX>, smem);
+      secondary_chain_kernel<CTXT_PARTS, LOG2_N_MAX><<<grid, CT, smem, st>>>(a);
+    } else {
+      set_smem(secondary_chain_kernel<CTXT_PARTS, 0>, smem);
+      secondary_chain_kernel<CTXT_PARTS, 0><<<grid, CT, smem, st>>>(a);
+    }
   }
 }
 
