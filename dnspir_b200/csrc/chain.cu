@@ -612,13 +612,14 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   a.qv_stride = qv_stride;
   a.nl = nq * CTXT_PARTS;
   a.out = out;
-  // one part per block while the chunk's blocks fit in one wave (they then
-  // share SMs with a running scan); three parts per block beyond that
+  // one part per block (80 KiB: two blocks per SM, or one beside a scan
+  // block) unless the chunk's blocks exceed two per SM; three parts per
+  // block beyond that
   int sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool full = g.log2n == LOG2_N_MAX;
-  if ((long)nq * CTXT_PARTS * g.H * 2 <= sms) {
+  if ((long)nq * CTXT_PARTS * g.H * 2 <= 2 * sms) {
     const size_t smem = chain_smem(g, 1);
     const dim3 grid(2, CTXT_PARTS * g.H, nq);
     if (full) {

@@ -84,13 +84,16 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
 }
 
 // One block: column r of half h for up to 8 lanes.
+constexpr int LIFT_LANES_CHAIN = 4;
+
 __global__ void encode_lift_kernel(const uint32_t* __restrict__ Ahat, uint32_t* __restrict__ out, Group g, int nl,
                                    int frame, uint32_t scale, const uint32_t* __restrict__ pow5inv,
                                    const uint32_t* __restrict__ gtab, NttTables T) {
   extern __shared__ uint32_t sm[];
   const uint32_t r = blockIdx.x, h = blockIdx.y;
-  const int lane0 = blockIdx.z * 8;
-  const int nlg = min(8, nl - lane0);
+  const int lpb = frame == 0 ? 8 : LIFT_LANES_CHAIN;  // lanes per block
+  const int lane0 = blockIdx.z * lpb;
+  const int nlg = min(lpb, nl - lane0);
   const uint32_t N = g.n;
   const int logn = g.log2n;
   uint32_t* x1 = sm;
@@ -214,9 +217,12 @@ void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int
   uint32_t linv = 1;
   for (uint32_t x = 1; x < TPLAIN; x++)
     if ((x * (g.l % TPLAIN)) % TPLAIN == 1) linv = x;
-  const int nlg = nl < 8 ? nl : 8;
+  // frame 0 writes the 8 lanes of a slot together; frame 1 (chain layout)
+  // takes fewer lanes per block so that three blocks fit on an SM
+  const int lpb = frame == 0 ? 8 : LIFT_LANES_CHAIN;
+  const int nlg = nl < lpb ? nl : lpb;
   const size_t smem = (size_t)2 * nlg * g.n * 4;
-  dim3 grid(g.L, g.H, (nl + 7) / 8);
+  dim3 grid(g.L, g.H, (nl + lpb - 1) / lpb);
   set_smem(encode_lift_kernel, smem);
   encode_lift_kernel<<<grid, 512, smem, st>>>(Ahat, out, g, nl, frame, linv, pow_table(g.log2n, true), maps.g, T);
 }

@@ -5,7 +5,8 @@
 // Queries are answered in groups of up to `batch`: one pass of the scan over
 // every shard serves the whole group (the slab is read once per group), then
 // the secondary databases are encoded and evaluated in chunks of one wave of
-// chain clusters (SMs / (2 H) queries, capped by a memory budget).  Two scan
+// chain clusters (two one-part blocks per SM: 2 SMs / (6 H) queries, capped by
+// a memory budget).  Two scan
 // engines: CUDA cores over the lane layout (groups of 1, 2, 4, 8 or 16) and
 // the tensor cores over the tensor layout (groups up to 256, tile shape per
 // group size from a table or from dnspir_fleet_tune).  Two buffer slots
@@ -278,12 +279,13 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   f->S = num_shards;
   f->D = num_distinct;
   {
-    // one wave of secondary chain clusters (one block per SM, 2 H per query)
+    // one wave of secondary chain clusters (one-part blocks, two per SM:
+    // 2 x 3 x H blocks per query)
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const Group& g2 = f->g2;
     const size_t per_query = ((size_t)2 * g2.H * g2.L + (size_t)g2.H * g2.L) * CTXT_PARTS * g2.n * 4;
-    const int wave = std::max(1, sms / (2 * (int)g2.H));
+    const int wave = std::max(1, 2 * sms / (2 * CTXT_PARTS * (int)g2.H));
     f->sec_chunk = (int)std::max<size_t>(1, std::min<size_t>(wave, SEC_BUDGET / per_query));
   }
   CK(cudaStreamCreateWithFlags(&f->own, cudaStreamNonBlocking));

@@ -30,121 +30,154 @@ __device__ __forceinline__ uint32_t brv(uint32_t i, int logn) { return logn ? (_
 
 __device__ __forceinline__ uint32_t prime_of(int pi) { return pi ? P2 : P1; }
 
-// Forward transform of `cnt` length-2^logn polynomials stored back to back in
-// shared memory; result slot s sits at position brv(s).  All threads of the
-// block must call; ends with __syncthreads().
-__device__ __forceinline__ void ntt_fwd_smem(uint32_t* x, int logn, int cnt, const NttTables& T, int pi) {
-  const uint32_t p = prime_of(pi);
-  const uint32_t* __restrict__ tw = T.fw[pi];
-  const uint32_t* __restrict__ twq = T.fwq[pi];
-  const int half = 1 << (logn - 1);
-  const int total = cnt << (logn - 1);
-  for (int s = 0; s < logn; s++) {
-    const int logt = logn - 1 - s;
-    const int t = 1 << logt;
-    const int m = 1 << s;
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int poly = b >> (logn - 1);
-      const int k = b & (half - 1);
-      const int i = k >> logt;
-      const int j = (i << (logt + 1)) + (k & (t - 1));
-      uint32_t* a = x + (poly << logn);
-      const uint32_t w = __ldg(tw + m + i), wq = __ldg(twq + m + i);
-      const uint32_t U = a[j];
-      const uint32_t V = shoup_mul(a[j + t], w, wq, p);
-      a[j] = add_mod(U, V, p);
-      a[j + t] = sub_mod(U, V, p);
-    }
-    __syncthreads();
-  }
+namespace ntt_detail {
+
+// Harvey's lazy butterflies with Shoup multiplication: a forward pass keeps
+// values in [0, 4p), an inverse pass in [0, 2p) (4p < 2^28).
+__device__ __forceinline__ uint32_t lazy_mul(uint32_t x, uint32_t w, uint32_t wq, uint32_t p) {
+  return x * w - __umulhi(x, wq) * p;  // in [0, 2p) for any x < 2^32
+}
+__device__ __forceinline__ uint32_t red(uint32_t x, uint32_t m) { return x >= m ? x - m : x; }
+__device__ __forceinline__ void ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
+  const uint32_t a = red(x, 2 * p);
+  const uint32_t t = lazy_mul(y, w, wq, p);
+  x = a + t;
+  y = a - t + 2 * p;
+}
+__device__ __forceinline__ void gs(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
+  const uint32_t a = x + y;
+  const uint32_t d = x - y + 2 * p;
+  x = red(a, 2 * p);
+  y = lazy_mul(d, w, wq, p);
 }
 
-// Inverse of ntt_fwd_smem: input slot s at position brv(s), output natural
-// coefficients (scaled by n^-1).  Ends with __syncthreads().
-__device__ __forceinline__ void ntt_inv_smem(uint32_t* x, int logn, int cnt, const NttTables& T, int pi) {
-  const uint32_t p = prime_of(pi);
-  const uint32_t* __restrict__ tw = T.iw[pi];
-  const uint32_t* __restrict__ twq = T.iwq[pi];
-  const int half = 1 << (logn - 1);
-  const int total = cnt << (logn - 1);
-  for (int s = 0; s < logn; s++) {
-    const int t = 1 << s;
-    const int h = half >> s;
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int poly = b >> (logn - 1);
-      const int k = b & (half - 1);
-      const int i = k >> s;
-      const int j = (i << (s + 1)) + (k & (t - 1));
-      uint32_t* a = x + (poly << logn);
-      const uint32_t w = __ldg(tw + h + i), wq = __ldg(twq + h + i);
-      const uint32_t U = a[j], V = a[j + t];
-      a[j] = add_mod(U, V, p);
-      a[j + t] = shoup_mul(sub_mod(U, V, p), w, wq, p);
+// cnt0 polynomials with factor 0 followed by cnt1 with factor 1, back to back,
+// radix-4 passes (one barrier per two stages) and a radix-2 pass for odd logn.
+__device__ __forceinline__ void fwd(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
+  const int n = 1 << logn, cnt = cnt0 + cnt1;
+  int s = 0;
+  for (; s + 1 < logn; s += 2) {
+    const int logt2 = logn - s - 2;
+    const int t2 = 1 << logt2, t = 2 * t2, m = 1 << s;
+    const int total = cnt << (logn - 2);
+    for (int gg = threadIdx.x; gg < total; gg += blockDim.x) {
+      const int poly = gg >> (logn - 2), g = gg & ((n >> 2) - 1);
+      const int pi = poly >= cnt0;
+      const uint32_t p = prime_of(pi);
+      const uint32_t* __restrict__ tw = T.fw[pi];
+      const uint32_t* __restrict__ twq = T.fwq[pi];
+      const int blk = g >> logt2, r = g & (t2 - 1);
+      uint32_t* a = x + (poly << logn) + (blk << (logt2 + 2)) + r;
+      uint32_t v0 = a[0], v1 = a[t2], v2 = a[t], v3 = a[t + t2];
+      const uint32_t w = __ldg(tw + m + blk), wq = __ldg(twq + m + blk);
+      ct(v0, v2, w, wq, p);
+      ct(v1, v3, w, wq, p);
+      ct(v0, v1, __ldg(tw + 2 * m + 2 * blk), __ldg(twq + 2 * m + 2 * blk), p);
+      ct(v2, v3, __ldg(tw + 2 * m + 2 * blk + 1), __ldg(twq + 2 * m + 2 * blk + 1), p);
+      a[0] = v0, a[t2] = v1, a[t] = v2, a[t + t2] = v3;
     }
     __syncthreads();
   }
-  const uint32_t ni = T.ninv[pi][logn], niq = T.ninvq[pi][logn];
-  const int n_all = cnt << logn;
-  for (int b = threadIdx.x; b < n_all; b += blockDim.x) x[b] = shoup_mul(x[b], ni, niq, p);
+  if (s < logn) {  // last stage, t = 1; outputs brought to [0, p)
+    const int total = cnt << (logn - 1);
+    for (int bb = threadIdx.x; bb < total; bb += blockDim.x) {
+      const int poly = bb >> (logn - 1), b = bb & ((n >> 1) - 1);
+      const int pi = poly >= cnt0;
+      const uint32_t p = prime_of(pi);
+      uint32_t* a = x + (poly << logn) + 2 * b;
+      uint32_t u = a[0], v = a[1];
+      ct(u, v, __ldg(T.fw[pi] + n / 2 + b), __ldg(T.fwq[pi] + n / 2 + b), p);
+      a[0] = red(red(u, 2 * p), p);
+      a[1] = red(red(v, 2 * p), p);
+    }
+  } else {
+    const int total = cnt << logn;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const uint32_t p = prime_of((b >> logn) >= cnt0);
+      x[b] = red(red(x[b], 2 * p), p);
+    }
+  }
   __syncthreads();
+}
+
+__device__ __forceinline__ void inv(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
+  const int n = 1 << logn, cnt = cnt0 + cnt1;
+  int s = 0;
+  for (; s + 1 < logn; s += 2) {
+    const int t = 1 << s;
+    const int h0 = n >> (s + 1), h1 = n >> (s + 2);
+    const int total = cnt << (logn - 2);
+    for (int gg = threadIdx.x; gg < total; gg += blockDim.x) {
+      const int poly = gg >> (logn - 2), g = gg & ((n >> 2) - 1);
+      const int pi = poly >= cnt0;
+      const uint32_t p = prime_of(pi);
+      const uint32_t* __restrict__ tw = T.iw[pi];
+      const uint32_t* __restrict__ twq = T.iwq[pi];
+      const int blk = g >> s, r = g & (t - 1);
+      uint32_t* a = x + (poly << logn) + (blk << (s + 2)) + r;
+      uint32_t v0 = a[0], v1 = a[t], v2 = a[2 * t], v3 = a[3 * t];
+      gs(v0, v1, __ldg(tw + h0 + 2 * blk), __ldg(twq + h0 + 2 * blk), p);
+      gs(v2, v3, __ldg(tw + h0 + 2 * blk + 1), __ldg(twq + h0 + 2 * blk + 1), p);
+      const uint32_t w = __ldg(tw + h1 + blk), wq = __ldg(twq + h1 + blk);
+      gs(v0, v2, w, wq, p);
+      gs(v1, v3, w, wq, p);
+      a[0] = v0, a[t] = v1, a[2 * t] = v2, a[3 * t] = v3;
+    }
+    __syncthreads();
+  }
+  if (s < logn) {  // last stage, t = n/2
+    const int total = cnt << (logn - 1);
+    for (int jj = threadIdx.x; jj < total; jj += blockDim.x) {
+      const int poly = jj >> (logn - 1), j = jj & ((n >> 1) - 1);
+      const int pi = poly >= cnt0;
+      const uint32_t p = prime_of(pi);
+      uint32_t* a = x + (poly << logn) + j;
+      uint32_t u = a[0], v = a[n / 2];
+      gs(u, v, __ldg(T.iw[pi] + 1), __ldg(T.iwq[pi] + 1), p);
+      a[0] = u;
+      a[n / 2] = v;
+    }
+    __syncthreads();
+  }
+  // scale by n^-1 and bring to [0, p)
+  const int total = cnt << logn;
+  for (int b = threadIdx.x; b < total; b += blockDim.x) {
+    const int pi = (b >> logn) >= cnt0;
+    const uint32_t p = prime_of(pi);
+    x[b] = red(lazy_mul(x[b], T.ninv[pi][logn], T.ninvq[pi][logn], p), p);
+  }
+  __syncthreads();
+}
+
+}  // namespace ntt_detail
+
+// Forward transform of `cnt` length-2^logn polynomials stored back to back in
+// shared memory; input in [0, p), result slot s at position brv(s), in
+// [0, p).  All threads of the block must call; ends with __syncthreads().
+__device__ __forceinline__ void ntt_fwd_smem(uint32_t* x, int logn, int cnt, const NttTables& T, int pi) {
+  if (pi)
+    ntt_detail::fwd(x, logn, 0, cnt, T);
+  else
+    ntt_detail::fwd(x, logn, cnt, 0, T);
+}
+
+// Inverse of ntt_fwd_smem: input slot s at position brv(s), in [0, p); output
+// natural coefficients scaled by n^-1, in [0, p).  Ends with __syncthreads().
+__device__ __forceinline__ void ntt_inv_smem(uint32_t* x, int logn, int cnt, const NttTables& T, int pi) {
+  if (pi)
+    ntt_detail::inv(x, logn, 0, cnt, T);
+  else
+    ntt_detail::inv(x, logn, cnt, 0, T);
 }
 
 // The same two transforms with the prime chosen per polynomial: polys
 // [0, cnt0) use factor 0 and [cnt0, cnt0 + cnt1) factor 1, in one set of
-// stages (halves the number of barriers when both factors are transformed).
+// passes (halves the number of barriers when both factors are transformed).
 __device__ __forceinline__ void ntt_fwd_smem2(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
-  const int half = 1 << (logn - 1);
-  const int cnt = cnt0 + cnt1;
-  const int total = cnt << (logn - 1);
-  for (int s = 0; s < logn; s++) {
-    const int logt = logn - 1 - s;
-    const int t = 1 << logt;
-    const int m = 1 << s;
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int poly = b >> (logn - 1);
-      const int pi = poly >= cnt0;
-      const uint32_t p = prime_of(pi);
-      const int k = b & (half - 1);
-      const int i = k >> logt;
-      const int j = (i << (logt + 1)) + (k & (t - 1));
-      uint32_t* a = x + (poly << logn);
-      const uint32_t w = __ldg(T.fw[pi] + m + i), wq = __ldg(T.fwq[pi] + m + i);
-      const uint32_t U = a[j];
-      const uint32_t V = shoup_mul(a[j + t], w, wq, p);
-      a[j] = add_mod(U, V, p);
-      a[j + t] = sub_mod(U, V, p);
-    }
-    __syncthreads();
-  }
+  ntt_detail::fwd(x, logn, cnt0, cnt1, T);
 }
 __device__ __forceinline__ void ntt_inv_smem2(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
-  const int half = 1 << (logn - 1);
-  const int cnt = cnt0 + cnt1;
-  const int total = cnt << (logn - 1);
-  for (int s = 0; s < logn; s++) {
-    const int t = 1 << s;
-    const int h = half >> s;
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int poly = b >> (logn - 1);
-      const int pi = poly >= cnt0;
-      const uint32_t p = prime_of(pi);
-      const int k = b & (half - 1);
-      const int i = k >> s;
-      const int j = (i << (s + 1)) + (k & (t - 1));
-      uint32_t* a = x + (poly << logn);
-      const uint32_t w = __ldg(T.iw[pi] + h + i), wq = __ldg(T.iwq[pi] + h + i);
-      const uint32_t U = a[j], V = a[j + t];
-      a[j] = add_mod(U, V, p);
-      a[j + t] = shoup_mul(sub_mod(U, V, p), w, wq, p);
-    }
-    __syncthreads();
-  }
-  const int n_all = cnt << logn;
-  for (int b = threadIdx.x; b < n_all; b += blockDim.x) {
-    const int pi = (b >> logn) >= cnt0;
-    x[b] = shoup_mul(x[b], T.ninv[pi][logn], T.ninvq[pi][logn], prime_of(pi));
-  }
-  __syncthreads();
+  ntt_detail::inv(x, logn, cnt0, cnt1, T);
 }
 
 }  // namespace dnspir
