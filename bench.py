@@ -84,6 +84,42 @@ def parse():
     return ap.parse_args()
 
 
+class RankGroup:
+    """The ranks of a torchrun launch: replicas, one GPU each, whose only
+    collectives are a barrier around the timed region and the max of the
+    per-rank times (no data-path collective)."""
+
+    def __init__(self, pg, device):
+        self.pg = pg
+        self.device = device
+
+    @classmethod
+    def init(cls, backend, world, timeout_s=600):
+        if world <= 1:
+            return cls(None, "cpu")
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+        return cls(tdist, "cuda" if backend == "nccl" else "cpu")
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, max_seconds):
+    """Units all ranks processed / the slowest rank's time."""
+    return units_per_rank * world / max_seconds
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
 
@@ -355,23 +391,9 @@ def main():
     import dnspir_b200 as dp
 
     torch.cuda.set_device(local_rank)
-    pg = None
-    if world > 1:
-        import torch.distributed as tdist
-        from datetime import timedelta
-        tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
-        pg = tdist
-
-    def barrier():
-        if pg:
-            pg.barrier()
-
-    def max_over_ranks(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    ranks = RankGroup.init("nccl", world)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
+    pg = ranks.pg
 
     dev = torch.device("cuda", local_rank)
     l1, l2, shards = dp.get_database_shape(args.entries)
@@ -517,7 +539,7 @@ def main():
                 return 1
             gscan = [float(bt[3, g * B]) for g in range(args.batched_groups)]
             batched[str(B)] = {
-                "responses_per_sec": nq * world / (bms * 1e-3), "groups": args.batched_groups,
+                "responses_per_sec": whole_job_rate(nq, world, bms * 1e-3), "groups": args.batched_groups,
                 "p50_ms": float(np.median(bt[0])), "p99_ms": float(np.percentile(bt[0], 99)),
                 "scan_ms_per_group": statistics.mean(gscan),
                 "effective_scan_gbs": B * (shards * slab_bytes) / (statistics.mean(gscan) * 1e-3) / 1e9,
@@ -534,7 +556,7 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     kname = "tscan_kernel" if args.engine == "tensor" else "scan_batch_kernel"
     traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_plain_2p22.md")
-    value = args.steps * world / (total_ms * 1e-3)
+    value = whole_job_rate(args.steps, world, total_ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -560,7 +582,7 @@ def main():
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": algo_bytes},
-        "e2e": {"value": args.steps * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": qlen,
+        "e2e": {"value": whole_job_rate(args.steps, world, e2e_s), "unit": UNIT, "h2d_bytes_per_step": qlen,
                 "d2h_bytes_per_step": dp.reply_bytes()},
         "gpu_launches": (9 if args.engine == "tensor" else 8) * args.steps,
         "clocks": clk,
