@@ -401,11 +401,13 @@ void launch_retile(const uint32_t* lane_slab, uint8_t* tensor_slab, const Group&
 
 // The tile shapes: queries per CTA (NQ / 4) and m-tiles per CTA.
 const TScanShape* tscan_shapes(int* count) {
-  // stages chosen so that the shapes with 1 m-tile and up to 128 rows fit two
-  // CTAs per SM
+  // stages chosen so that most shapes fit two CTAs per SM (one CTA's TMEM
+  // epilogue then overlaps the other's main loop); a few deeper one-per-SM
+  // variants for the tuner to compare
   static const TScanShape shapes[] = {
-      {16, 1, 5},  {16, 1, 10}, {32, 1, 5},  {64, 1, 4},  {64, 2, 3},  {128, 1, 3},
-      {128, 2, 3}, {256, 1, 3}, {256, 1, 4}, {256, 2, 2}, {256, 2, 3}, {512, 1, 2},
+      {16, 1, 5},  {16, 1, 10}, {32, 1, 5},  {64, 1, 4},  {64, 2, 3},  {64, 2, 2},
+      {128, 1, 3}, {128, 2, 2}, {128, 2, 3}, {256, 1, 2}, {256, 1, 3}, {256, 1, 4},
+      {256, 2, 2}, {256, 2, 3}, {512, 1, 2},
   };
   *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
   return shapes;
