@@ -89,6 +89,8 @@ def lib():
         L.dnspir_fleet_tune.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_tscan_shapes.argtypes = [_vp, _vp, _vp, c.c_int]
         L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
+        L.dnspir_fleet_set_tile.argtypes = [_vp, c.c_uint32, c.c_int]
+        L.dnspir_fleet_tune_pipeline.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
         L.dnspir_server_add_db.argtypes = [_vp, _vp, c.c_uint32, _u32p]
         L.dnspir_server_start.argtypes = [_vp, c.c_int]
@@ -381,17 +383,23 @@ class Fleet:
         [nq][6][2][N] natural NTT order, out [nq][shards][2][N][8]."""
         _check(lib().dnspir_fleet_scan(self._h, _dev_ptr(qnat), qnat.shape[0], _dev_ptr(out)))
 
+    def set_tile(self, batch, shape_index):
+        """Tensor engine: tile shape index for groups of `batch` (-1: default)."""
+        _check(lib().dnspir_fleet_set_tile(self._h, batch, shape_index))
+
     def set_engine(self, engine):
         """ENGINE_CUDA_CORES or ENGINE_TENSOR; marks every shard unprepared."""
         _check(lib().dnspir_fleet_set_engine(self._h, engine))
 
-    def tune(self, batch):
+    def tune(self, batch, pipeline=False):
         """Tensor engine: time each tile shape for groups of `batch` queries and
-        keep the fastest.  Returns (chosen index, ms per shape, shapes)."""
+        keep the fastest (pipeline=True: whole groups through both phases
+        instead of the scan alone).  Returns (chosen index, ms per shape, shapes)."""
         shapes = tscan_shapes()
         ms = np.full(len(shapes), -1.0)
         chosen = ctypes.c_int(-1)
-        _check(lib().dnspir_fleet_tune(self._h, batch, _ptr(ms), ctypes.byref(chosen)))
+        fn = lib().dnspir_fleet_tune_pipeline if pipeline else lib().dnspir_fleet_tune
+        _check(fn(self._h, batch, _ptr(ms), ctypes.byref(chosen)))
         return chosen.value, ms, shapes
 
     def set_stream(self, stream_handle):

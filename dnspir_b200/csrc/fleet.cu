@@ -434,6 +434,88 @@ int dnspir_fleet_tune(dnspir_fleet* f, uint32_t batch, double* ms_per_shape, int
   return DNSPIR_OK;
 }
 
+int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_shape, int* chosen) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  uint64_t qlen = 0;
+  {
+    std::lock_guard<std::mutex> lk(f->mu);
+    NOT_SERVING(f);
+    if (f->engine != DNSPIR_ENGINE_TENSOR) return fail(DNSPIR_ERR_BAD_ARG, "tuning applies to the tensor engine");
+    if (batch < 1 || batch > (uint32_t)TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
+    if (f->g1.log2n != LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_SHAPE, "the wire format is defined for N = 2048");
+    CKR(fleet_ready(f));
+    qlen = dnspir_query_bytes(f->g1.l, f->g2.l);
+  }
+  DeviceGuard dg(f->device);
+  // zero query bytes (valid wire data) answered in three groups per shape:
+  // the first warms up, the other two are timed through both phases
+  const int nb = (int)batch, groups = 3;
+  const size_t RB = dnspir_reply_bytes();
+  DBuf q, r;
+  CKR(q.ensure((size_t)nb * groups * qlen));
+  CKR(r.ensure((size_t)nb * groups * RB));
+  CK(cudaMemset(q.p, 0, (size_t)nb * groups * qlen));
+  std::vector<const uint8_t*> ptrs(nb * groups);
+  std::vector<uint64_t> lens(nb * groups, qlen);
+  for (int i = 0; i < nb * groups; i++) ptrs[i] = q.as<uint8_t>() + (size_t)i * qlen;
+  const int old_batch = f->batch;
+  const auto old_tuned = f->tuned;
+  f->batch = nb;
+  int count = 0;
+  const TScanShape* sh = tscan_shapes(&count);
+  double best = 1e30;
+  int best_i = -1;
+  int rc = DNSPIR_OK;
+  for (int i = 0; i < count && rc == DNSPIR_OK; i++) {
+    const int qg = sh[i].nq / 4;
+    const int pad = (nb + qg - 1) / qg * qg;
+    double ms = -1;
+    // candidates: padding at most a factor 2, and at most 8 query groups per m-tile
+    if ((pad <= 2 * nb || qg <= 4) && qg * 8 >= nb) {
+      f->tuned[nb] = i;
+      rc = dnspir_fleet_process_queries(f, ptrs.data(), lens.data(), (uint32_t)(nb * groups), r.as<uint8_t>(), RB,
+                                        nullptr, 1);
+      if (rc == DNSPIR_OK) {
+        std::lock_guard<std::mutex> lk(f->mu);
+        float t = 0;
+        cudaEvent_t* t1 = &f->tev[6];
+        cudaEvent_t* t2 = &f->tev[12];
+        if (cudaEventElapsedTime(&t, t1[0], t2[5]) == cudaSuccess) ms = t / 2;
+        cudaGetLastError();
+      }
+    }
+    if (ms_per_shape) ms_per_shape[i] = ms;
+    if (ms > 0 && ms < best) {
+      best = ms;
+      best_i = i;
+    }
+  }
+  f->batch = old_batch;
+  f->tuned = old_tuned;
+  if (rc != DNSPIR_OK) return rc;
+  if (best_i < 0) return fail(DNSPIR_ERR_CUDA, "no tile shape ran");
+  f->tuned[nb] = best_i;
+  if (chosen) *chosen = best_i;
+  return DNSPIR_OK;
+}
+
+int dnspir_fleet_set_tile(dnspir_fleet* f, uint32_t batch, int shape_index) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
+  if (f->engine != DNSPIR_ENGINE_TENSOR) return fail(DNSPIR_ERR_BAD_ARG, "tiles apply to the tensor engine");
+  if (batch < 1 || batch > (uint32_t)TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
+  int count = 0;
+  tscan_shapes(&count);
+  if (shape_index < 0) {
+    f->tuned.erase((int)batch);
+    return DNSPIR_OK;
+  }
+  if (shape_index >= count) return fail(DNSPIR_ERR_BAD_ARG, "no such tile shape");
+  f->tuned[(int)batch] = shape_index;
+  return DNSPIR_OK;
+}
+
 int dnspir_fleet_scan(dnspir_fleet* f, const uint32_t* qnat_dev, uint32_t nq, uint32_t* out_dev) {
   if (!f || (nq && (!qnat_dev || !out_dev))) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(f->mu);

@@ -138,6 +138,16 @@ int dnspir_fleet_tune(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape,
  * = evaluation at zeta^-(2k+1)); out: [query][shard][factor][slot u][lane]
  * with slot u = (sign, e) for 2k+1 = +-5^e mod 2N, u = sign * N/2 + e. */
 int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, uint32_t* out);
+/* The same, timing whole groups (decode, scan, epilogue, secondary phase,
+ * replies; zero query bytes, two timed groups after one warm-up) instead of
+ * the scan alone: the shape that maximises responses/s when the secondary
+ * phase of one group overlaps the scan of the next.  ms_per_shape receives
+ * milliseconds per group. */
+int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
+/* Tensor engine: use tile shape `shape_index` (dnspir_tscan_shapes order) for
+ * groups of `batch` queries, overriding the table or a previous tune; -1
+ * returns to the default.  No counterpart in the reference. */
+int dnspir_fleet_set_tile(dnspir_fleet* fleet, uint32_t batch, int shape_index);
 /* The tensor scan's tile shapes (query-operand rows per CTA, m-tiles per CTA,
  * pipeline stages); returns their count. */
 int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int max);

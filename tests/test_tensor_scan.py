@@ -129,3 +129,20 @@ def test_tensor_engine_shape_rules():
     assert e.value.code == 7
     with pytest.raises(dp.DnspirError):
         g.set_batch(257)
+
+
+def test_tensor_tune_pipeline_keeps_replies(config1_pair):
+    # the whole-group tuner times shapes with zero queries, then real replies
+    # of the tuned group size still equal the oracle's
+    data, fa, fb, refs, l1, l2, shards = config1_pair
+    chosen, ms, shapes = fb.tune(6, pipeline=True)
+    assert 0 <= chosen < len(shapes) and ms[chosen] > 0
+    rng = orc.Rng(bytes([8]) + bytes(31))
+    qs = [orc.prepare_query(rng, (97 * k) % 8192, k % shards, l1, l2) for k in range(6)]
+    fb.set_batch(6)
+    try:
+        got = fb.process_queries([q for q, _ in qs])
+    finally:
+        fb.set_batch(1)
+    for (q, seed), r in zip(qs, got):
+        assert r == orc.process_query(refs, q)
