@@ -216,6 +216,9 @@ def run_serve(args, rank, local_rank):
     sizes = [1 << 15, 1 << 18, 1 << 20, 1 << 22]
     shares = [float(x) for x in args.serve_mix.split(",")]
     batch_cap = {1 << 15: 256, 1 << 18: 256, 1 << 20: 128, 1 << 22: 64}
+    # batching window (min pending queries, max wait ms): cheap databases wait
+    # briefly for fuller groups instead of launching near-empty ones
+    batch_window = {1 << 15: (32, 4.0), 1 << 18: (16, 8.0), 1 << 20: (8, 16.0), 1 << 22: (1, 0.0)}
     fleets, shapes, distinct = [], [], []
     t0 = time.time()
     for e in sizes:
@@ -254,6 +257,8 @@ def run_serve(args, rank, local_rank):
     for rate in [float(r) for r in args.serve_rate.split(",")]:
         sv = dp.Server(max_sessions=2 * args.serve_clients * len(sizes), device=local_rank)
         ids = [sv.add_db(f, batch_cap[e]) for f, e in zip(fleets, sizes)]
+        for i, e in zip(ids, sizes):
+            sv.set_batching(i, *batch_window[e])
         sv.start(graphs=True)
         sessions = [[sv.open_session(q[:gk]) if c % 2 else -1 for c, (q, _, _, _) in enumerate(pool)]
                     for pool in pools]

@@ -94,6 +94,7 @@ def lib():
         L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
         L.dnspir_server_add_db.argtypes = [_vp, _vp, c.c_uint32, _u32p]
         L.dnspir_server_start.argtypes = [_vp, c.c_int]
+        L.dnspir_server_set_batching.argtypes = [_vp, c.c_uint32, c.c_uint32, c.c_uint32]
         L.dnspir_server_open_session.argtypes = [_vp, c.c_char_p, c.c_uint64, _u64p]
         L.dnspir_server_close_session.argtypes = [_vp, c.c_uint64]
         L.dnspir_server_submit.argtypes = [_vp, c.c_uint32, c.c_int64, c.c_char_p, c.c_uint64, _u64p]
@@ -428,6 +429,11 @@ class Server:
         _check(lib().dnspir_server_add_db(self._h, fleet._h, max_batch, ctypes.byref(i)))
         self._fleets.append(fleet)
         return i.value
+
+    def set_batching(self, db, min_batch, max_wait_ms):
+        """Hold a database's group until min_batch queries are pending or the
+        oldest has waited max_wait_ms."""
+        _check(lib().dnspir_server_set_batching(self._h, db, min_batch, int(max_wait_ms * 1000)))
 
     def start(self, graphs=True):
         _check(lib().dnspir_server_start(self._h, 1 if graphs else 0))

@@ -18,7 +18,13 @@
 //   * completion is observed with event queries; replies are copied out of
 //     the slot's pinned buffer and the request is marked done.
 // Group sizes are admitted by free device memory: a database's group size is
-// halved until its two slots and the secondary workspace fit.  Sessions keep
+// halved until its two slots and the secondary workspace fit.  Each database
+// gets its own pair of streams for the session, prioritised by database size
+// (smaller databases first, and within a database the secondary phase above
+// the scans), so short groups of small databases are dispatched between the
+// blocks of long scans of large ones.  An optional batching window per
+// database holds a group until it has min_batch queries or its oldest query
+// has waited max_wait, so that cheap databases do not launch near-empty groups.  Sessions keep
 // a client's decoded Galois keys on the device; a query of a session omits the
 // two key polynomials from its bytes.
 #include <algorithm>
@@ -58,6 +64,10 @@ struct InFlight {
 
 struct Db {
   dnspir_fleet* f = nullptr;
+  cudaStream_t saved_st = nullptr, saved_sec = nullptr;  // the fleet's own streams, restored at stop
+  cudaStream_t st = nullptr, sec = nullptr;              // serving streams (priority by database size)
+  int min_batch = 1;                                     // batching window: launch at this many pending
+  double max_wait_s = 0;                                 // ... or when the oldest has waited this long
   int max_batch = 1;  // requested
   int admitted = 1;   // after memory admission
   int bk_max = 1;
@@ -261,6 +271,12 @@ void worker_main(dnspir_server* sv) {
       std::vector<uint64_t> tk;
       {
         std::lock_guard<std::mutex> lk(sv->mu);
+        // batching window: wait for min_batch pending queries unless the
+        // oldest has waited max_wait_s (or the server is draining)
+        if ((int)db.pending.size() < std::min(db.min_batch, db.admitted) && sv->running.load()) {
+          auto it = db.pending.empty() ? sv->reqs.end() : sv->reqs.find(db.pending.front());
+          if (it == sv->reqs.end() || now_s() - it->second.t_submit < db.max_wait_s) continue;
+        }
         while (!db.pending.empty() && (int)rq.size() < db.admitted) {
           const uint64_t t = db.pending.front();
           db.pending.pop_front();
@@ -344,6 +360,16 @@ int dnspir_server_add_db(dnspir_server* sv, dnspir_fleet* f, uint32_t max_batch,
   return DNSPIR_OK;
 }
 
+int dnspir_server_set_batching(dnspir_server* sv, uint32_t db_id, uint32_t min_batch, uint32_t max_wait_us) {
+  if (!sv) return fail(DNSPIR_ERR_BAD_ARG, "null server");
+  if (db_id >= sv->dbs.size()) return fail(DNSPIR_ERR_BAD_ARG, "no such database");
+  if (min_batch < 1) return fail(DNSPIR_ERR_BAD_ARG, "min_batch must be at least 1");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->dbs[db_id]->min_batch = (int)min_batch;
+  sv->dbs[db_id]->max_wait_s = max_wait_us * 1e-6;
+  return DNSPIR_OK;
+}
+
 int dnspir_server_start(dnspir_server* sv, int use_graphs) {
   if (!sv) return fail(DNSPIR_ERR_BAD_ARG, "null server");
   if (sv->running.load()) return fail(DNSPIR_ERR_BAD_ARG, "already running");
@@ -369,7 +395,27 @@ int dnspir_server_start(dnspir_server* sv, int use_graphs) {
     }
     CKR(presize(db));
     for (auto& s : f->slot) s.drop_graphs();
-    f->serving = true;
+  }
+  {
+    // serving streams: rank databases by slab words per query (smallest first);
+    // each database's secondary phase above its own scans
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    std::vector<size_t> order(sv->dbs.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    auto work = [&](size_t i) { return (double)sv->dbs[i]->f->S * slab_words(sv->dbs[i]->f->g1); };
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return work(a) < work(b); });
+    for (size_t k = 0; k < order.size(); k++) {
+      Db& db = *sv->dbs[order[k]];
+      const int p_sec = std::min(least, greatest + 2 * (int)k), p_st = std::min(least, greatest + 2 * (int)k + 1);
+      CK(cudaStreamCreateWithPriority(&db.sec, cudaStreamNonBlocking, p_sec));
+      CK(cudaStreamCreateWithPriority(&db.st, cudaStreamNonBlocking, p_st));
+      db.saved_st = db.f->st;
+      db.saved_sec = db.f->sec;
+      db.f->st = db.st;
+      db.f->sec = db.sec;
+      db.f->serving = true;
+    }
   }
   CK(cudaDeviceSynchronize());
   sv->running = true;
@@ -532,6 +578,13 @@ int dnspir_server_stop(dnspir_server* sv) {
       s.drop_graphs();
       s.sec_pending = false;
       s.prim_recorded = false;
+    }
+    if (dbp->saved_st) {
+      f->st = dbp->saved_st;
+      f->sec = dbp->saved_sec;
+      cudaStreamDestroy(dbp->st);
+      cudaStreamDestroy(dbp->sec);
+      dbp->st = dbp->sec = dbp->saved_st = dbp->saved_sec = nullptr;
     }
     f->serving = false;
   }

@@ -169,6 +169,11 @@ typedef struct dnspir_server dnspir_server;
 int dnspir_server_create(int device, uint32_t max_sessions, dnspir_server** out);
 /* max_batch: 1..256 (tensor engine) or 1, 2, 4, 8, 16 (CUDA cores). */
 int dnspir_server_add_db(dnspir_server* server, dnspir_fleet* fleet, uint32_t max_batch, uint32_t* db_id);
+/* Batching window of a database (default 1 query, no wait): a group launches
+ * once min_batch queries are pending or the oldest has waited max_wait_us. */
+int dnspir_server_set_batching(dnspir_server* server, uint32_t db_id, uint32_t min_batch, uint32_t max_wait_us);
+/* Databases are served on streams of their own, prioritised by database size
+ * (smaller first); the fleets get their own streams back at stop. */
 int dnspir_server_start(dnspir_server* server, int use_graphs);
 int dnspir_server_open_session(dnspir_server* server, const uint8_t* galois_key_bytes, uint64_t len,
                                uint64_t* session);

@@ -67,6 +67,7 @@ def test_served_mix_equals_alone(two_dbs):
     sv = dp.Server(max_sessions=4)
     ida = sv.add_db(fa, 8)
     idb = sv.add_db(fb, 4)
+    sv.set_batching(ida, 3, 20.0)  # database a holds groups for up to 3 queries or 20 ms
     sv.start(graphs=True)
     try:
         # two clients of database a use sessions: keys sent once, then short queries
