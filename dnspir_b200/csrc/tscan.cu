@@ -247,10 +247,10 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
     cw[5] = reduce64(cw[4] << 8, pr, mu);
     cw[6] = reduce64(cw[5] << 8, pr, mu);
     const int k = lane & 3, l8 = lane >> 2;
-    const uint64_t c0 = k == 0 ? cw[0] : k == 1 ? cw[1] : k == 2 ? cw[2] : cw[3];
-    const uint64_t c1 = k == 0 ? cw[1] : k == 1 ? cw[2] : k == 2 ? cw[3] : cw[4];
-    const uint64_t c2 = k == 0 ? cw[2] : k == 1 ? cw[3] : k == 2 ? cw[4] : cw[5];
-    const uint64_t c3 = k == 0 ? cw[3] : k == 1 ? cw[4] : k == 2 ? cw[5] : cw[6];
+    const uint32_t c0 = (uint32_t)(k == 0 ? cw[0] : k == 1 ? cw[1] : k == 2 ? cw[2] : cw[3]);
+    const uint32_t c1 = (uint32_t)(k == 0 ? cw[1] : k == 1 ? cw[2] : k == 2 ? cw[3] : cw[4]);
+    const uint32_t c2 = (uint32_t)(k == 0 ? cw[2] : k == 1 ? cw[3] : k == 2 ? cw[4] : cw[5]);
+    const uint32_t c3 = (uint32_t)(k == 0 ? cw[3] : k == 1 ? cw[4] : k == 2 ? cw[5] : cw[6]);  // 2^(8w) mod p < 2^26
     const uint32_t N = 2 * a.half;
     for (int t = 0; t < MTPC; t++) {
       const uint32_t u = sgn * a.half + 4 * (mt0 + t) + warp;
