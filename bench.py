@@ -514,6 +514,7 @@ def main():
             if args.engine == "tensor":
                 ch, tms, shapes = fleet.tune(B, pipeline=True)
                 shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
+                         "persistent": bool(shapes[ch][3]),
                          "tuned_ms_per_group": round(float(tms[ch]), 3), "tuner": "whole-group pipeline"}
             fleet.set_batch(B)
             nq = B * max(2, args.batched_groups)

@@ -87,7 +87,7 @@ def lib():
         L.dnspir_fleet_set_batch.argtypes = [_vp, c.c_uint32]
         L.dnspir_fleet_set_engine.argtypes = [_vp, c.c_int]
         L.dnspir_fleet_tune.argtypes = [_vp, c.c_uint32, _vp, _vp]
-        L.dnspir_tscan_shapes.argtypes = [_vp, _vp, _vp, c.c_int]
+        L.dnspir_tscan_shapes.argtypes = [_vp, _vp, _vp, _vp, c.c_int]
         L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
         L.dnspir_fleet_set_tile.argtypes = [_vp, c.c_uint32, c.c_int]
         L.dnspir_fleet_tune_pipeline.argtypes = [_vp, c.c_uint32, _vp, _vp]
@@ -259,9 +259,10 @@ ENGINE_TENSOR = 1
 
 
 def tscan_shapes():
-    """The tensor scan's tile shapes: (query-operand rows, m-tiles, stages) per CTA."""
-    n = lib().dnspir_tscan_shapes(None, None, None, 0)
-    a = [np.zeros(n, dtype=np.int32) for _ in range(3)]
+    """The tensor scan's tile shapes: (query-operand rows, m-tiles, stages,
+    persistent) per CTA."""
+    n = lib().dnspir_tscan_shapes(None, None, None, None, 0)
+    a = [np.zeros(n, dtype=np.int32) for _ in range(4)]
     lib().dnspir_tscan_shapes(*[_ptr(x) for x in a], n)
     return [tuple(int(x[i]) for x in a) for i in range(n)]
 

@@ -65,11 +65,12 @@ const TScanShape& tensor_shape(dnspir_fleet* f, int nb, int* nb_pad) {
   if (it != f->tuned.end()) {
     idx = it->second;
   } else {
-    // untuned: the narrowest query tile that holds the group, one m-tile
+    // untuned: the narrowest query tile that holds the group, one m-tile,
+    // the one-tile-per-CTA kernel
     const int want = nb <= 4 ? 16 : nb <= 8 ? 32 : nb <= 16 ? 64 : nb <= 32 ? 128 : nb <= 64 ? 256 : 512;
     idx = 0;
     for (int i = count - 1; i >= 0; i--)
-      if (sh[i].nq == want && sh[i].mtpc == 1) idx = i;
+      if (sh[i].nq == want && sh[i].mtpc == 1 && !sh[i].persistent) idx = i;
   }
   const int q = sh[idx].nq / 4;
   *nb_pad = (nb + q - 1) / q * q;
@@ -539,13 +540,14 @@ int dnspir_fleet_scan(dnspir_fleet* f, const uint32_t* qnat_dev, uint32_t nq, ui
   return fleet_drain(f);
 }
 
-int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int max) {
+int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int* persistent, int max) {
   int count = 0;
   const TScanShape* sh = tscan_shapes(&count);
   for (int i = 0; i < count && i < max; i++) {
     if (nq) nq[i] = sh[i].nq;
     if (mtpc) mtpc[i] = sh[i].mtpc;
     if (stages) stages[i] = sh[i].stages;
+    if (persistent) persistent[i] = sh[i].persistent;
   }
   return count;
 }

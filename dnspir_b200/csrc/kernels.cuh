@@ -88,9 +88,10 @@ int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* q
 // [p][sign][m-tile][k-chunk] (same size as the lane layout).  Needs loop_len
 // = N/2 and N >= 256.
 struct TScanShape {
-  int nq;      // rows of the query operand per CTA (4 limbs x queries)
-  int mtpc;    // 128-row m-tiles per CTA
-  int stages;  // shared-memory pipeline depth
+  int nq;          // rows of the query operand per CTA (4 limbs x queries)
+  int mtpc;        // 128-row m-tiles per CTA
+  int stages;      // shared-memory pipeline depth
+  int persistent;  // 1: persistent warp-specialised kernel, double-buffered TMEM
 };
 int tensor_layout_supported(const Group& g);
 void tensor_dims(const Group& g, uint32_t* mt_total, uint32_t* kc_total);

@@ -28,6 +28,8 @@
 // their 32 TMEM lanes and write the reduced residues.  Every wait is bounded;
 // a wait that gives up sets an error word, and the CTA still waits for its
 // copies in flight and frees its TMEM before returning.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace dnspir {
@@ -290,6 +292,215 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
   }
 }
 
+// ---- persistent, warp-specialised variant.  Warp 0 streams the A and V
+// chunks of every tile the CTA owns (tiles blockIdx.x, + gridDim.x, ...)
+// through the stage ring; warp 1 issues the MMAs of tile j into TMEM
+// accumulator j mod 2; warps 2..5 read accumulator j mod 2 (TMEM lane quarter
+// warp mod 4) and write the residues, then release it, so the epilogue of
+// tile j overlaps the main loop of tile j + 1.  Needs 2 x MTPC x NQ <= 512
+// TMEM columns.  Waits are bounded as in tscan_kernel; a role that gives up
+// raises the abort flag, and the CTA still waits for its MMAs and copies in
+// flight before it frees TMEM.
+constexpr int TSCANP_NT = 192;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(bar)) : "memory");
+}
+
+template <int NQ, int MTPC>
+__global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
+  constexpr uint32_t A_BYTES = MTPC * TBLK;
+  constexpr uint32_t STAGE = A_BYTES + NQ * 128;
+  constexpr uint32_t ACC = MTPC * NQ;  // TMEM columns of one accumulator
+  constexpr uint32_t COLS = 2 * ACC;
+  static_assert(STAGE % 1024 == 0 && ACC >= 16 && COLS <= 512 && (COLS & (COLS - 1)) == 0, "tile shape");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t S_ = a.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + S_ * STAGE);
+  uint64_t* empty = full + S_;
+  uint64_t* accf = empty + S_;  // [2] accumulator ready (MMA commit)
+  uint64_t* acce = accf + 2;    // [2] accumulator drained (4 epilogue warps)
+  uint64_t* done = acce + 2;    // every MMA of the CTA complete
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile uint32_t* issued_s = tslot + 1;
+  volatile uint32_t* consumed_s = tslot + 2;
+  volatile uint32_t* abort_s = tslot + 3;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const uint32_t mtc = a.mt_total / MTPC;
+  const uint32_t items = (uint32_t)a.nshards * 4 * mtc * a.groups;
+  const uint32_t KC = a.kc_total;
+
+  if (threadIdx.x == 0) {
+    for (uint32_t i = 0; i < S_; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    mbar_init(done, 1);
+    *issued_s = 0;
+    *consumed_s = 0;
+    *abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(tslot)), "r"(COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  auto tile_of = [&](uint32_t item, uint32_t& grp, uint32_t& mt0, uint32_t& sgn, int& p, int& s) {
+    grp = item % a.groups;
+    item /= a.groups;
+    mt0 = (item % mtc) * MTPC;
+    item /= mtc;
+    sgn = item & 1;
+    p = (item >> 1) & 1;
+    s = item >> 2;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t g = 0;
+      for (uint32_t item = blockIdx.x; item < items && !*abort_s; item += gridDim.x) {
+        uint32_t grp, mt0, sgn;
+        int p, s;
+        tile_of(item, grp, mt0, sgn, p, s);
+        const size_t ps = (size_t)p * 2 + sgn;
+        const uint8_t* abase = a.slabs[s] + (ps * a.mt_total + mt0) * KC * TBLK;
+        const uint8_t* bbase = a.qb + ps * KC * a.nq_rows * 128 + (size_t)grp * NQ * 128;
+        for (uint32_t kc = 0; kc < KC; kc++, g++) {
+          const uint32_t st = g % S_, n = g / S_;
+          if (n > 0 && !mbar_wait(&empty[st], (n - 1) & 1)) {
+            *abort_s = 1;
+            atomicOr(a.err, 1u);
+            break;
+          }
+          uint8_t* dst = sm + st * STAGE;
+          mbar_expect_tx(&full[st], STAGE);
+#pragma unroll
+          for (int t = 0; t < MTPC; t++)
+            bulk_g2s(dst + t * TBLK, abase + ((size_t)t * KC + kc) * TBLK, TBLK, &full[st]);
+          bulk_g2s(dst + A_BYTES, bbase + (size_t)kc * a.nq_rows * 128, NQ * 128, &full[st]);
+          *issued_s = g + 1;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_u8(128, NQ);
+      uint32_t g = 0, j = 0;
+      for (uint32_t item = blockIdx.x; item < items && !*abort_s; item += gridDim.x, j++) {
+        const uint32_t buf = j & 1, use = j >> 1;
+        if (use > 0 && !mbar_wait(&acce[buf], (use - 1) & 1)) {
+          *abort_s = 1;
+          atomicOr(a.err, 1u);
+          break;
+        }
+        tc_fence_after();
+        bool ok = true;
+        for (uint32_t kc = 0; kc < KC; kc++, g++) {
+          const uint32_t st = g % S_, n = g / S_;
+          if (!mbar_wait(&full[st], n & 1)) {
+            *abort_s = 1;
+            atomicOr(a.err, 1u);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t s0 = sa(sm + st * STAGE);
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int t = 0; t < MTPC; t++)
+              mma_u8(tmem + buf * ACC + t * NQ, sw128_desc(s0 + t * TBLK + 32 * k), sw128_desc(s0 + A_BYTES + 32 * k),
+                     idesc, (kc | k) != 0);
+          mma_commit(&empty[st]);
+          *consumed_s = g + 1;
+        }
+        if (!ok) break;
+        mma_commit(&accf[buf]);
+      }
+      mma_commit(done);
+    }
+  } else {
+    const int q = warp & 3;  // TMEM lane quarter = slot e mod 4 of the m-tile
+    const int k = lane & 3, l8 = lane >> 2;
+    const uint32_t N = 2 * a.half;
+    uint32_t j = 0;
+    for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, j++) {
+      const uint32_t buf = j & 1, use = j >> 1;
+      if (!mbar_wait(&accf[buf], use & 1)) {
+        if (lane == 0) {
+          *abort_s = 1;
+          atomicOr(a.err, 1u);
+        }
+        break;
+      }
+      tc_fence_after();
+      uint32_t grp, mt0, sgn;
+      int p, s;
+      tile_of(item, grp, mt0, sgn, p, s);
+      const uint32_t pr = prime_of(p);
+      const uint64_t mu = barrett_mu(pr);
+      const uint64_t c32 = reduce64(1ull << 32, pr, mu);
+      const uint64_t c40 = reduce64(c32 << 8, pr, mu);
+      const uint64_t c48 = reduce64(c40 << 8, pr, mu);
+      // c_w = 2^(8w) mod p < 2^26 for w = k .. k + 3
+      const uint32_t w3 = (uint32_t)reduce64(1ull << 24, pr, mu);
+      const uint32_t c0 = k == 0 ? 1u : k == 1 ? 256u : k == 2 ? 65536u : w3;
+      const uint32_t c1 = k == 0 ? 256u : k == 1 ? 65536u : k == 2 ? w3 : (uint32_t)c32;
+      const uint32_t c2 = k == 0 ? 65536u : k == 1 ? w3 : k == 2 ? (uint32_t)c32 : (uint32_t)c40;
+      const uint32_t c3 = k == 0 ? w3 : k == 1 ? (uint32_t)c32 : k == 2 ? (uint32_t)c40 : (uint32_t)c48;
+      for (int t = 0; t < MTPC; t++) {
+        const uint32_t u = sgn * a.half + 4 * (mt0 + t) + q;
+#pragma unroll 1
+        for (int q4 = 0; q4 < NQ / 16; q4++) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ + 16 * q4, v);
+          uint64_t tot[4];
+#pragma unroll
+          for (int qq = 0; qq < 4; qq++) {
+            uint64_t x = (uint64_t)v[4 * qq] * c0 + (uint64_t)v[4 * qq + 1] * c1 + (uint64_t)v[4 * qq + 2] * c2 +
+                         (uint64_t)v[4 * qq + 3] * c3;
+            x += __shfl_xor_sync(0xffffffffu, x, 1);
+            x += __shfl_xor_sync(0xffffffffu, x, 2);
+            tot[qq] = x;
+          }
+          const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
+          const uint32_t bq = grp * (NQ / 4) + 4 * q4 + k;
+          if (bq < a.nvalid)
+            a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[buf]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 32) mbar_wait(done, 0);  // every MMA issued by the CTA has completed
+  if (threadIdx.x == 0) {
+    // copies issued but never consumed (only after a wait gave up) must land
+    // before the shared memory is released
+    for (uint32_t g = *consumed_s; g < *issued_s; g++) mbar_wait(&full[g % S_], (g / S_) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+  }
+}
+
 // Lane layout (slab_off) -> tensor layout; one thread per 16-byte unit.
 __global__ void retile_kernel(const uint32_t* __restrict__ src, uint8_t* __restrict__ dst, Group g, uint32_t mt_total,
                               uint32_t kc_total) {
@@ -383,6 +594,28 @@ int launch_t(const TScanArgs& a0, int stages, cudaStream_t st) {
   return 0;
 }
 
+template <int NQ, int MTPC>
+int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
+  TScanArgs a = a0;
+  a.stages = (uint32_t)stages;
+  constexpr uint32_t STAGE = MTPC * TBLK + NQ * 128;
+  const size_t smem = 1024 + (size_t)stages * STAGE + (2 * stages + 5) * 8 + 16;
+  if (smem > 227 * 1024) return -1;
+  set_smem(tscanp_kernel<NQ, MTPC>, smem);
+  constexpr int COLS = 2 * MTPC * NQ;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tscanp_kernel<NQ, MTPC>, TSCANP_NT, smem);
+  // resident CTAs must not ask for more TMEM columns than the SM has (a CTA
+  // whose allocation waits would hold its SM until a neighbour finishes)
+  if (per_sm < 1 || per_sm * COLS > 512) return -1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t items = (size_t)a.nshards * 4 * (a.mt_total / MTPC) * a.groups;
+  const size_t grid = std::min(items, (size_t)sms * per_sm);
+  tscanp_kernel<NQ, MTPC><<<(unsigned)grid, TSCANP_NT, smem, st>>>(a);
+  return 0;
+}
+
 }  // namespace
 
 int tensor_layout_supported(const Group& g) { return g.log2n >= 8 && g.L == g.n / 2 && g.H >= 1; }
@@ -404,10 +637,13 @@ const TScanShape* tscan_shapes(int* count) {
   // stages chosen so that most shapes fit two CTAs per SM (one CTA's TMEM
   // epilogue then overlaps the other's main loop); a few deeper one-per-SM
   // variants for the tuner to compare
+  // (last field 1: the persistent warp-specialised kernel, stages sized so
+  // that resident CTAs never exceed the SM's 512 TMEM columns)
   static const TScanShape shapes[] = {
-      {16, 1, 5},  {16, 1, 10}, {32, 1, 5},  {64, 1, 4},  {64, 2, 3},  {64, 2, 2},
-      {128, 1, 3}, {128, 2, 2}, {128, 2, 3}, {256, 1, 2}, {256, 1, 3}, {256, 1, 4},
-      {256, 2, 2}, {256, 2, 3}, {512, 1, 2},
+      {16, 1, 5, 0},  {16, 1, 10, 0}, {32, 1, 5, 0},  {64, 1, 4, 0},  {64, 2, 3, 0},  {64, 2, 2, 0},
+      {128, 1, 3, 0}, {128, 2, 2, 0}, {128, 2, 3, 0}, {256, 1, 2, 0}, {256, 1, 3, 0}, {256, 1, 4, 0},
+      {256, 2, 2, 0}, {256, 2, 3, 0}, {512, 1, 2, 0}, {16, 1, 6, 1},  {64, 1, 5, 1},  {64, 2, 4, 1},
+      {128, 1, 4, 1}, {128, 2, 3, 1}, {256, 1, 3, 1}, {256, 1, 4, 1},
   };
   *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
   return shapes;
@@ -444,6 +680,17 @@ int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, s
   a.groups = nb_pad / qpc;
   a.stages = 0;
   const int stg = shape.stages;
+  if (shape.persistent) {
+    switch (shape.nq * 10 + shape.mtpc) {
+      case 161: return launch_tp<16, 1>(a, stg, st);
+      case 641: return launch_tp<64, 1>(a, stg, st);
+      case 642: return launch_tp<64, 2>(a, stg, st);
+      case 1281: return launch_tp<128, 1>(a, stg, st);
+      case 1282: return launch_tp<128, 2>(a, stg, st);
+      case 2561: return launch_tp<256, 1>(a, stg, st);
+      default: return -1;
+    }
+  }
   switch (shape.nq * 10 + shape.mtpc) {
     case 161: return launch_t<16, 1>(a, stg, st);
     case 321: return launch_t<32, 1>(a, stg, st);

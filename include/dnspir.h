@@ -149,8 +149,9 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_p
  * returns to the default.  No counterpart in the reference. */
 int dnspir_fleet_set_tile(dnspir_fleet* fleet, uint32_t batch, int shape_index);
 /* The tensor scan's tile shapes (query-operand rows per CTA, m-tiles per CTA,
- * pipeline stages); returns their count. */
-int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int max);
+ * pipeline stages, 1 for the persistent warp-specialised kernel); returns
+ * their count. */
+int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int* persistent, int max);
 
 /* ---- Serving loop (no counterpart in the reference, whose server answers each
  * connection on its own thread with process_query, dns/server.rs:789).

@@ -146,3 +146,20 @@ def test_tensor_tune_pipeline_keeps_replies(config1_pair):
         fb.set_batch(1)
     for (q, seed), r in zip(qs, got):
         assert r == orc.process_query(refs, q)
+
+
+def test_every_tile_shape_equals_cuda_core_scan(config1_pair):
+    # each tile shape of the tensor scan, the persistent warp-specialised
+    # kernel included, forced for a group of 10 queries
+    torch = pytest.importorskip("torch")
+    data, fa, fb, refs, l1, l2, shards = config1_pair
+    q = _qnat(torch, 10, 2048, 4242)
+    want = _scan(torch, fa, q, shards, 2048)
+    fb.set_batch(10)
+    try:
+        for i, shape in enumerate(dp.tscan_shapes()):
+            fb.set_tile(10, i)
+            assert np.array_equal(_scan(torch, fb, q, shards, 2048), want), shape
+    finally:
+        fb.set_tile(10, -1)
+        fb.set_batch(1)
