@@ -354,12 +354,17 @@ __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane
 // the block needs 128 KiB and shares an SM with a scan block (latency: the
 // chains of a few queries overlap the next scan).  The key constants gk_a0,
 // gk_a1, qry_a, gk_b0, gk_b1, qry_b (Montgomery form) and the sigma_5
-// destinations of a thread's positions live in its registers.  Shared memory
-// (u32 words):
-//   FW FWQ IW IWQ             4N   twiddles of this factor
-//   per part: A TC D X0 X1 B  6N   a, saved sigma_5(a), work vector, published iNTT x2, b
-// (4 + 6 LN) N words: 176 KiB for LN = 3, 80 KiB for LN = 1 at N = 2048.
-constexpr int SEC_PART_WORDS = 6;  // x N
+// destinations of a thread's positions live in its registers.  Each step's
+// pointwise stage writes the next step's sigma_5-permuted a and b straight
+// into the other buffer of a pair, and the inverse transform is published to
+// the peer from its own buffer D[i mod 2] (the peer reads it between the
+// cluster barriers of steps i and i + 1; this block rewrites it only at the end
+// of step i + 1).  Shared memory (u32 words):
+//   FW FWQ IW IWQ                    4N   twiddles of this factor
+//   per part: TC[2] D[2] B[2] H      7N   sigma_5(a) kept, sigma_5(a) transformed
+//                                         (published), sigma_5(b), high digit
+// (4 + 7 LN) N words: 200 KiB for LN = 3, 88 KiB for LN = 1 at N = 2048.
+constexpr int SEC_PART_WORDS = 7;  // x N
 __host__ __device__ constexpr int sec_smem_words(int ln) { return 4 + ln * SEC_PART_WORDS; }
 
 template <int LN, int LOGN>
@@ -376,7 +381,8 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
   uint32_t* IWQ = IW + N;
   uint32_t* P0 = IWQ + N;  // part blocks
   const int PS = SEC_PART_WORDS * N;
-  const int oTC = N, oD = 2 * N, oX = 3 * N, oB = 5 * N;
+  // per part: TC[2] at 0, N; D[2] at 2N, 3N; B[2] at 4N, 5N; H at 6N
+  const int oTC = 0, oD = 2 * N, oB = 4 * N, oH = 6 * N;
   const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
   constexpr int PER = N_MAX / CT;  // positions per thread (N <= N_MAX)
   uint32_t kc[6][PER], dst[PER];
@@ -400,62 +406,41 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
     IW[b] = a.T.iw[p][b];
     IWQ[b] = a.T.iwq[p][b];
 #pragma unroll
-    for (int t = 0; t < LN; t++) {
-      P0[t * PS + b] = 0;
+    for (int t = 0; t < LN; t++) {  // a = b = 0, so sigma_5(a) = sigma_5(b) = 0
+      P0[t * PS + oTC + b] = 0;
+      P0[t * PS + oD + b] = 0;
       P0[t * PS + oB + b] = 0;
     }
   }
   cluster.sync();
   const uint32_t* peer = cluster.map_shared_rank(P0, p ^ 1);
   for (uint32_t i = 0; i < a.g.L; i++) {
+    const int cur = (int)(i & 1) * N, nxt = N - cur;
     // entries of row i (the three parts' lanes are adjacent), consumed at the end of the step
     const uint32_t* Ei = a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + (size_t)q * CTXT_PARTS + part0) * N;
-    uint32_t e[LN][PER], ra[LN][PER], rb[LN][PER];
+    uint32_t e[LN][PER];
 #pragma unroll
     for (int t = 0; t < LN; t++)
 #pragma unroll
       for (int c = 0; c < PER; c++) {
         const int pos = threadIdx.x + c * CT;
         e[t][c] = pos < N ? __ldg(Ei + (size_t)t * N + pos) : 0;
-        if (pos < N) {
-          ra[t][c] = P0[t * PS + pos];
-          rb[t][c] = P0[t * PS + oB + pos];
-        }
       }
-    __syncthreads();
-    // sigma_5 on a and b
-#pragma unroll
-    for (int c = 0; c < PER; c++) {
-      const int pos = threadIdx.x + c * CT;
-      if (pos < N) {
-#pragma unroll
-        for (int t = 0; t < LN; t++) {
-          P0[t * PS + oTC + dst[c]] = ra[t][c];
-          P0[t * PS + oD + dst[c]] = ra[t][c];
-          P0[t * PS + oB + dst[c]] = rb[t][c];
-        }
-      }
-    }
-    __syncthreads();
-    inv_multi<LN, LOGN>(P0 + oD, PS, logn, IW, IWQ, pr);
-    const int xo = oX + (int)(i & 1) * N;
-    for (int b = threadIdx.x; b < N; b += CT)
-#pragma unroll
-      for (int t = 0; t < LN; t++) P0[t * PS + xo + b] = P0[t * PS + oD + b];
+    inv_multi<LN, LOGN>(P0 + oD + cur, PS, logn, IW, IWQ, pr);
     cluster.sync();
     for (int b = threadIdx.x; b < N; b += CT) {
       uint32_t own[LN], other[LN];
 #pragma unroll
-      for (int t = 0; t < LN; t++) own[t] = P0[t * PS + oD + b], other[t] = peer[t * PS + xo + b];
+      for (int t = 0; t < LN; t++) own[t] = P0[t * PS + oD + cur + b], other[t] = peer[t * PS + oD + cur + b];
 #pragma unroll
       for (int t = 0; t < LN; t++) {
         const int32_t hd = p == 0 ? high_digit(own[t], other[t], a.cp[0], a.cp[1])
                                   : high_digit(other[t], own[t], a.cp[0], a.cp[1]);
-        P0[t * PS + oD + b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
+        P0[t * PS + oH + b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr) : (uint32_t)hd;
       }
     }
     __syncthreads();
-    fwd_multi<LN, LOGN>(P0 + oD, PS, logn, FW, FWQ, pr);
+    fwd_multi<LN, LOGN>(P0 + oH, PS, logn, FW, FWQ, pr);
 #pragma unroll
     for (int c = 0; c < PER; c++) {
       const int pos = threadIdx.x + c * CT;
@@ -465,22 +450,35 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
 #pragma unroll
         for (int t = 0; t < LN; t++) {
           uint32_t* P = P0 + t * PS;
-          const uint32_t n1 = P[oD + pos];
-          const uint32_t n0 = sub_mod(P[oTC + pos], mont_reduce((uint64_t)n1 * cp.c26, pr, cp.pinv), pr);
-          P[pos] = mont_reduce((uint64_t)n0 * cg0 + (uint64_t)n1 * cg1 + (uint64_t)e[t][c] * cqa, pr, cp.pinv);
-          P[oB + pos] = mont_reduce(((uint64_t)P[oB + pos] << 32) + (uint64_t)n0 * qg0 + (uint64_t)n1 * qg1 +
-                                        (uint64_t)e[t][c] * qqb,
-                                    pr, cp.pinv);
+          const uint32_t n1 = P[oH + pos];
+          const uint32_t n0 = sub_mod(P[oTC + cur + pos], mont_reduce((uint64_t)n1 * cp.c26, pr, cp.pinv), pr);
+          const uint32_t an =
+              mont_reduce((uint64_t)n0 * cg0 + (uint64_t)n1 * cg1 + (uint64_t)e[t][c] * cqa, pr, cp.pinv);
+          const uint32_t bn = mont_reduce(((uint64_t)P[oB + cur + pos] << 32) + (uint64_t)n0 * qg0 +
+                                              (uint64_t)n1 * qg1 + (uint64_t)e[t][c] * qqb,
+                                          pr, cp.pinv);
+          // sigma_5 for the next step
+          P[oTC + nxt + dst[c]] = an;
+          P[oD + nxt + dst[c]] = an;
+          P[oB + nxt + dst[c]] = bn;
         }
       }
     }
     __syncthreads();
   }
-  for (int bb = threadIdx.x; bb < LN * N; bb += CT) {
-    const int t = bb >> logn, b = bb & (N - 1);
-    uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + part0 + t) * 2) * 2 * N;
-    o[(size_t)p * N + b] = P0[t * PS + b];
-    o[2 * (size_t)N + (size_t)p * N + b] = P0[t * PS + oB + b];
+  // the state after the last step sits sigma_5-permuted in buffer L mod 2
+  const int fin = (int)(a.g.L & 1) * N;
+#pragma unroll
+  for (int c = 0; c < PER; c++) {
+    const int pos = threadIdx.x + c * CT;
+    if (pos < N) {
+#pragma unroll
+      for (int t = 0; t < LN; t++) {
+        uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + part0 + t) * 2) * 2 * N;
+        o[(size_t)p * N + pos] = P0[t * PS + oTC + fin + dst[c]];
+        o[2 * (size_t)N + (size_t)p * N + pos] = P0[t * PS + oB + fin + dst[c]];
+      }
+    }
   }
   cluster.sync();  // keep this block's shared memory alive until the peer's last read
 }
