@@ -498,7 +498,7 @@ def main():
     batched = {}
     sizes = [int(x) for x in args.batched.split(",") if x.strip()]
     if args.engine == "cuda":
-        sizes = [b for b in sizes if b in (1, 2, 4, 8, 16)]
+        sizes = [b for b in sizes if b <= 256 and b & (b - 1) == 0]
     if sizes:
         fleet.set_stream(stream.cuda_stream)
         pool_n = 2 * max(sizes)
@@ -516,6 +516,10 @@ def main():
                 shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
                          "persistent": bool(shapes[ch][3]),
                          "tuned_ms_per_group": round(float(tms[ch]), 3), "tuner": "whole-group pipeline"}
+            else:
+                pb, tms = fleet.tune_cuda_cores(B)
+                shape = {"queries_per_block": pb, "tuned_scan_ms": round(float(tms[[1, 2, 4, 8, 16].index(pb)]), 3),
+                         "tuner": "scan alone"}
             fleet.set_batch(B)
             nq = B * max(2, args.batched_groups)
             sel = torch.arange(nq, device=dev) % pool_n

@@ -91,6 +91,7 @@ def lib():
         L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
         L.dnspir_fleet_set_tile.argtypes = [_vp, c.c_uint32, c.c_int]
         L.dnspir_fleet_tune_pipeline.argtypes = [_vp, c.c_uint32, _vp, _vp]
+        L.dnspir_fleet_tune_cuda_cores.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
         L.dnspir_server_add_db.argtypes = [_vp, _vp, c.c_uint32, _u32p]
         L.dnspir_server_start.argtypes = [_vp, c.c_int]
@@ -376,7 +377,7 @@ class Fleet:
         return out[:, :n]
 
     def set_batch(self, max_batch):
-        """Queries per pass over the slabs (CUDA cores: 1, 2, 4, 8, 16; tensor
+        """Queries per pass over the slabs (CUDA cores: a power of two up to 256; tensor
         cores: 1..256); replies do not depend on it."""
         _check(lib().dnspir_fleet_set_batch(self._h, max_batch))
 
@@ -392,6 +393,15 @@ class Fleet:
     def set_engine(self, engine):
         """ENGINE_CUDA_CORES or ENGINE_TENSOR; marks every shard unprepared."""
         _check(lib().dnspir_fleet_set_engine(self._h, engine))
+        self._engine = engine
+
+    def tune_cuda_cores(self, batch):
+        """CUDA-core engine: time 1, 2, 4, 8, 16 queries per block for groups of
+        `batch` and keep the fastest.  Returns (queries per block, ms per tile)."""
+        ms = np.full(5, -1.0)
+        chosen = ctypes.c_int(-1)
+        _check(lib().dnspir_fleet_tune_cuda_cores(self._h, batch, _ptr(ms), ctypes.byref(chosen)))
+        return chosen.value, ms
 
     def tune(self, batch, pipeline=False):
         """Tensor engine: time each tile shape for groups of `batch` queries and

@@ -7,7 +7,7 @@
 // the secondary databases are encoded and evaluated in chunks of one wave of
 // chain clusters (two one-part blocks per SM: 2 SMs / (6 H) queries, capped by
 // a memory budget).  Two scan
-// engines: CUDA cores over the lane layout (groups of 1, 2, 4, 8 or 16) and
+// engines: CUDA cores over the lane layout (groups of a power of two up to 256) and
 // the tensor cores over the tensor layout (groups up to 256, tile shape per
 // group size from a table or from dnspir_fleet_tune).  Two buffer slots
 // alternate between groups: the primary phase of group k+1 (main stream) runs
@@ -116,8 +116,10 @@ int launch_scan(dnspir_fleet* f, QSlot& s, int nb, int Bk) {
   }
   if (Bk > nb)  // unused query positions of the kernel batch compute on zeros
     CK(cudaMemsetAsync(s.qnat.as<uint32_t>() + (size_t)nb * qv, 0, (size_t)(Bk - nb) * qv * 4, f->st));
-  if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), qv, Bk, s.fin.as<uint32_t>(), g1,
-                        slot_maps(f->ctx, g1.log2n), f->st))
+  auto it = f->tuned_cc.find(nb);
+  const int per_block = it == f->tuned_cc.end() ? 0 : std::min(it->second, Bk);
+  if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), qv, Bk, per_block,
+                        s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), f->st))
     return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
   return DNSPIR_OK;
 }
@@ -335,7 +337,7 @@ int dnspir_fleet_set_batch(dnspir_fleet* f, uint32_t max_batch) {
   if (f->engine == DNSPIR_ENGINE_TENSOR) {
     if (max_batch < 1 || max_batch > TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
   } else if (!scan_batch_supported((int)max_batch)) {
-    return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1, 2, 4, 8 or 16");
+    return fail(DNSPIR_ERR_BAD_ARG, "batch must be a power of two up to 256");
   }
   f->batch = (int)max_batch;
   return DNSPIR_OK;
@@ -359,6 +361,7 @@ int dnspir_fleet_set_engine(dnspir_fleet* f, int engine) {
   f->engine = engine;
   f->batch = 1;
   f->tuned.clear();
+  f->tuned_cc.clear();
   return DNSPIR_OK;
 }
 
@@ -497,6 +500,61 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
   if (best_i < 0) return fail(DNSPIR_ERR_CUDA, "no tile shape ran");
   f->tuned[nb] = best_i;
   if (chosen) *chosen = best_i;
+  return DNSPIR_OK;
+}
+
+int dnspir_fleet_tune_cuda_cores(dnspir_fleet* f, uint32_t batch, double* ms_per_tile, int* chosen) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
+  if (f->engine != DNSPIR_ENGINE_CUDA_CORES) return fail(DNSPIR_ERR_BAD_ARG, "this tuner applies to the CUDA-core engine");
+  if (!scan_batch_supported((int)batch)) return fail(DNSPIR_ERR_BAD_ARG, "batch must be a power of two up to 256");
+  CKR(fleet_ready(f));
+  DeviceGuard dg(f->device);
+  const Group& g1 = f->g1;
+  const size_t n = g1.n, qv = QV_WORDS_PER_QUERY * n;
+  const int B = (int)batch;
+  DBuf qnat, out;
+  CKR(qnat.ensure((size_t)B * qv * 4));
+  CKR(out.ensure((size_t)B * f->S * 2 * n * SIMD * 4));
+  CK(cudaMemsetAsync(qnat.p, 0, (size_t)B * qv * 4, f->st));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  static const int tiles[5] = {1, 2, 4, 8, 16};
+  double best = 1e30;
+  int best_t = -1;
+  for (int i = 0; i < 5; i++) {
+    double ms = -1;
+    if (tiles[i] <= B && tiles[i] * 16 >= B) {  // at most 16 groups per block row
+      float t = 0, tot = 0;
+      bool ok = true;
+      for (int r = 0; r < 3 && ok; r++) {
+        cudaEventRecord(e0, f->st);
+        ok = launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, qnat.as<uint32_t>(), qv, B, tiles[i],
+                               out.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), f->st) == 0;
+        cudaEventRecord(e1, f->st);
+        if (ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) {
+          if (r > 0) tot += t;
+        } else {
+          ok = false;
+        }
+      }
+      cudaGetLastError();
+      if (ok) ms = tot / 2;
+    }
+    if (ms_per_tile) ms_per_tile[i] = ms;
+    if (ms > 0 && ms < best) {
+      best = ms;
+      best_t = tiles[i];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaStreamSynchronize(f->st));
+  if (best_t < 0) return fail(DNSPIR_ERR_CUDA, "no tile ran");
+  f->tuned_cc[B] = best_t;
+  if (chosen) *chosen = best_t;
   return DNSPIR_OK;
 }
 

@@ -53,6 +53,7 @@ struct dnspir_fleet {
   bool serving = false;                       // attached to a running server
   dnspir::DBuf qb, err_word, tmp_lane;        // tensor engine: query operand, wait-error word, preprocessing scratch
   std::map<int, int> tuned;                   // tensor engine: group size -> tile shape index
+  std::map<int, int> tuned_cc;                // CUDA-core engine: group size -> queries per block
   std::vector<cudaEvent_t> tev;               // 6 timing events per group of the last call
   std::vector<int> q_group;                   // per query of the last call: its group, or -1
   std::mutex mu;

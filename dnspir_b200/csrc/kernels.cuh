@@ -77,12 +77,14 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
                             const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st);
 
 // ---- primary scan (main_pir_loop, base_pir.rs:1085-1247)
-// B queries (B in {1, 2, 4, 8, 16}) per pass over all shards.  qnat: per query
-// [slot][p][N] natural order (slots 0 gk0, 1 gk1, 2 pq, 3 pqc), q_stride words
-// apart.  out: [b][s][p][u][lane] reduced mod p.
+// B queries (a power of two up to 256) in one launch over all shards, each
+// block serving per_block of them (1, 2, 4, 8 or 16; 0: min(B, 16)), the other
+// groups of per_block on grid.y.  qnat: per query [slot][p][N] natural order
+// (slots 0 gk0, 1 gk1, 2 pq, 3 pqc), q_stride words apart.  out:
+// [b][s][p][u][lane] reduced mod p.
 int scan_batch_supported(int B);
 int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int B,
-                      uint32_t* out, const Group& g, const SlotMaps& maps, cudaStream_t st);
+                      int per_block, uint32_t* out, const Group& g, const SlotMaps& maps, cudaStream_t st);
 // ---- primary scan on the tensor cores (tscan.cu): 8-bit limbs, kind::i8
 // Tensor layout: the slab indexed by query slot, bytes in 128 x 128 blocks
 // [p][sign][m-tile][k-chunk] (same size as the lane layout).  Needs loop_len

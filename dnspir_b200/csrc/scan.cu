@@ -63,6 +63,8 @@ __global__ void __launch_bounds__(SCAN_NT) scan_batch_kernel(ScanArgs a) {
   const size_t arr = (size_t)N * SIMD, row_stride = 3 * arr;
   // item = ((s * 2 + p) * 2 + sgn) * tiles + tile
   const uint32_t item = blockIdx.x;
+  // grid.y: which group of B queries of the kernel batch this block serves
+  const size_t qbase = (size_t)blockIdx.y * B;
   const uint32_t tile = item % tiles;
   const uint32_t sgn = (item / tiles) & 1;
   const int p = (item / (2 * tiles)) & 1;
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(SCAN_NT) scan_batch_kernel(ScanArgs a) {
         const uint32_t x = idx % Wr, b = (idx / Wr) % B, v = idx / (B * Wr);
         const uint32_t uu = sgn * half + (w0 + x) % half;
         const uint32_t kk = (__ldg(a.gtab + uu) - 1) >> 1;
-        win[(v * B + b) * W + x] = __ldg(a.qnat + b * a.q_stride + ((size_t)vslot[v] * 2 + p) * N + kk);
+        win[(v * B + b) * W + x] = __ldg(a.qnat + (qbase + b) * a.q_stride + ((size_t)vslot[v] * 2 + p) * N + kk);
       }
       __syncthreads();
       if (active) {
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(SCAN_NT) scan_batch_kernel(ScanArgs a) {
   if (active) {
 #pragma unroll
     for (int b = 0; b < B; b++) {
-      uint32_t* o = a.out + ((((size_t)b * a.nshards + s) * 2 + p) * N + u) * SIMD + lg * LPT;
+      uint32_t* o = a.out + ((((qbase + b) * a.nshards + s) * 2 + p) * N + u) * SIMD + lg * LPT;
 #pragma unroll
       for (int l = 0; l < LPT; l++) o[l] = reduce64(acc[l][b], pr, mu);
     }
@@ -233,13 +235,13 @@ __global__ void epilogue_zq_kernel(const uint32_t* __restrict__ part, int chunks
 }
 
 template <int B, int LPT>
-void launch_batch(const ScanArgs& a, cudaStream_t st) {
+void launch_batch(const ScanArgs& a, int groups, cudaStream_t st) {
   constexpr int TS = SCAN_NT / (SIMD / LPT);
   const size_t smem = (size_t)3 * (TS + a.rows - 1) * B * 4;
   set_smem(scan_batch_kernel<B, LPT>, smem);
   const uint32_t tiles = (a.g.n / 2 + TS - 1) / TS;
   const uint32_t items = (uint32_t)a.nshards * 4 * tiles;
-  scan_batch_kernel<B, LPT><<<items, SCAN_NT, smem, st>>>(a);
+  scan_batch_kernel<B, LPT><<<dim3(items, groups), SCAN_NT, smem, st>>>(a);
 }
 
 }  // namespace
@@ -253,10 +255,14 @@ static uint32_t inv5_of(uint32_t two_n) {
   return 1;
 }
 
-int scan_batch_supported(int B) { return B == 1 || B == 2 || B == 4 || B == 8 || B == 16; }
+int scan_batch_supported(int B) { return B >= 1 && B <= 256 && (B & (B - 1)) == 0; }
 
 int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int B,
-                      uint32_t* out, const Group& g, const SlotMaps& maps, cudaStream_t st) {
+                      int per_block, uint32_t* out, const Group& g, const SlotMaps& maps, cudaStream_t st) {
+  if (!scan_batch_supported(B)) return -1;
+  if (per_block <= 0) per_block = B < 16 ? B : 16;
+  if (per_block > B || B % per_block) return -1;
+  const int groups = B / per_block;
   ScanArgs a;
   a.g = g;
   a.slabs = slabs_dev;
@@ -266,12 +272,12 @@ int launch_scan_batch(uint32_t* const* slabs_dev, int nshards, const uint32_t* q
   a.gtab = maps.g;
   a.out = out;
   a.rows = (int)(g.L < 256 ? g.L : 256);
-  switch (B) {
-    case 1: launch_batch<1, 8>(a, st); break;
-    case 2: launch_batch<2, 8>(a, st); break;
-    case 4: launch_batch<4, 8>(a, st); break;
-    case 8: launch_batch<8, 4>(a, st); break;
-    case 16: launch_batch<16, 2>(a, st); break;
+  switch (per_block) {
+    case 1: launch_batch<1, 8>(a, groups, st); break;
+    case 2: launch_batch<2, 8>(a, groups, st); break;
+    case 4: launch_batch<4, 8>(a, groups, st); break;
+    case 8: launch_batch<8, 4>(a, groups, st); break;
+    case 16: launch_batch<16, 2>(a, groups, st); break;
     default: return -1;
   }
   return 0;

@@ -348,7 +348,7 @@ int dnspir_server_add_db(dnspir_server* sv, dnspir_fleet* f, uint32_t max_batch,
     std::lock_guard<std::mutex> lk(f->mu);
     CKR(fleet_ready(f));
   }
-  const int maxb = f->engine == DNSPIR_ENGINE_TENSOR ? 256 : 16;
+  const int maxb = 256;
   if (max_batch < 1 || (int)max_batch > maxb) return fail(DNSPIR_ERR_BAD_ARG, "max_batch out of range for the engine");
   if (f->engine == DNSPIR_ENGINE_CUDA_CORES && (max_batch & (max_batch - 1)))
     return fail(DNSPIR_ERR_BAD_ARG, "the CUDA-core engine takes power-of-two groups");

@@ -107,8 +107,8 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
  * dns/server.rs:707-728).  entries: count x (8 primary_order N) coefficients. */
 int dnspir_fleet_set_shards(dnspir_fleet* fleet, uint32_t first_distinct, uint32_t count, const uint16_t* entries,
                             int entries_on_device);
-/* Queries answered per pass over the shard slabs (default 1): 1, 2, 4, 8 or
- * 16 on the CUDA-core engine, 1..256 on the tensor engine.
+/* Queries answered per pass over the shard slabs (default 1): a power of two up
+ * to 256 on the CUDA-core engine, 1..256 on the tensor engine.
  * dnspir_fleet_process_queries splits its queries into groups of this size;
  * every group reads each slab once.  Replies do not depend on it.  The
  * reference answers one query per pass (process_queries, pir_wrapper.rs:349
@@ -144,6 +144,11 @@ int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, ui
  * phase of one group overlaps the scan of the next.  ms_per_shape receives
  * milliseconds per group. */
 int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
+/* CUDA-core engine: time the scan of a group of `batch` queries (a power of two
+ * up to 256, one launch) with 1, 2, 4, 8 and 16 queries per block and keep the
+ * fastest; ms_per_tile[5] receives the times (-1 when not run), *chosen the
+ * queries per block.  No counterpart in the reference. */
+int dnspir_fleet_tune_cuda_cores(dnspir_fleet* fleet, uint32_t batch, double* ms_per_tile, int* chosen);
 /* Tensor engine: use tile shape `shape_index` (dnspir_tscan_shapes order) for
  * groups of `batch` queries, overriding the table or a previous tune; -1
  * returns to the default.  No counterpart in the reference. */
@@ -168,7 +173,7 @@ int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int* persistent, int ma
  * with a session omits those bytes.  max_sessions may be 0. */
 typedef struct dnspir_server dnspir_server;
 int dnspir_server_create(int device, uint32_t max_sessions, dnspir_server** out);
-/* max_batch: 1..256 (tensor engine) or 1, 2, 4, 8, 16 (CUDA cores). */
+/* max_batch: 1..256 (tensor engine) or a power of two up to 256 (CUDA cores). */
 int dnspir_server_add_db(dnspir_server* server, dnspir_fleet* fleet, uint32_t max_batch, uint32_t* db_id);
 /* Batching window of a database (default 1 query, no wait): a group launches
  * once min_batch queries are pending or the oldest has waited max_wait_us. */

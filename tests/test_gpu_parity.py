@@ -220,3 +220,27 @@ def test_batched_group_with_rejected_query(config1):
     assert rc == 1 and list(status) == [0, 1, 0, 0]
     for k in (0, 2, 3):
         assert out[k].tobytes() == orc.process_query(refs, queries[k])
+
+
+@pytest.mark.parametrize("batch", [32, 64])
+def test_cuda_core_engine_large_groups(config1, batch):
+    # groups beyond 16 on the CUDA-core engine: one launch, blocks of 16 (or
+    # the tuned number of) queries on the second grid dimension
+    data, refs, fleet, l1, l2, shards = config1
+    rng = orc.Rng(bytes([5, batch]) + bytes(30))
+    n = batch + 3
+    qs = [orc.prepare_query(rng, (331 * k) % 8192, k % shards, l1, l2) for k in range(n)]
+    fleet.set_batch(batch)
+    try:
+        got = fleet.process_queries([q for q, _ in qs])
+        per_block, ms = fleet.tune_cuda_cores(batch)
+        assert per_block in (1, 2, 4, 8, 16) and ms.max() > 0
+        again = fleet.process_queries([q for q, _ in qs])
+    finally:
+        fleet.set_batch(1)
+    for k, ((q, seed), r) in enumerate(zip(qs, got)):
+        assert r == again[k]
+        if k % 7 == 0:
+            assert r == orc.process_query(refs, q), k
+            i, j = (331 * k) % 8192, k % shards
+            assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64))
