@@ -53,9 +53,14 @@ __device__ __forceinline__ void gs(uint32_t& x, uint32_t& y, uint32_t w, uint32_
 
 // cnt0 polynomials with factor 0 followed by cnt1 with factor 1, back to back,
 // radix-4 passes (one barrier per two stages) and a radix-2 pass for odd logn.
-__device__ __forceinline__ void fwd(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
+// LOGN > 0 fixes the length at compile time (stage loops unroll, every index
+// shift is a constant); the public entry points take that path for N = 2048.
+template <int LOGN>
+__device__ __forceinline__ void fwd_t(uint32_t* x, int logn_rt, int cnt0, int cnt1, const NttTables& T) {
+  const int logn = LOGN ? LOGN : logn_rt;
   const int n = 1 << logn, cnt = cnt0 + cnt1;
   int s = 0;
+#pragma unroll
   for (; s + 1 < logn; s += 2) {
     const int logt2 = logn - s - 2;
     const int t2 = 1 << logt2, t = 2 * t2, m = 1 << s;
@@ -100,9 +105,12 @@ __device__ __forceinline__ void fwd(uint32_t* x, int logn, int cnt0, int cnt1, c
   __syncthreads();
 }
 
-__device__ __forceinline__ void inv(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
+template <int LOGN>
+__device__ __forceinline__ void inv_t(uint32_t* x, int logn_rt, int cnt0, int cnt1, const NttTables& T) {
+  const int logn = LOGN ? LOGN : logn_rt;
   const int n = 1 << logn, cnt = cnt0 + cnt1;
   int s = 0;
+#pragma unroll
   for (; s + 1 < logn; s += 2) {
     const int t = 1 << s;
     const int h0 = n >> (s + 1), h1 = n >> (s + 2);
@@ -147,6 +155,19 @@ __device__ __forceinline__ void inv(uint32_t* x, int logn, int cnt0, int cnt1, c
     x[b] = red(lazy_mul(x[b], T.ninv[pi][logn], T.ninvq[pi][logn], p), p);
   }
   __syncthreads();
+}
+
+__device__ __forceinline__ void fwd(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
+  if (logn == LOG2_N_MAX)
+    fwd_t<LOG2_N_MAX>(x, logn, cnt0, cnt1, T);
+  else
+    fwd_t<0>(x, logn, cnt0, cnt1, T);
+}
+__device__ __forceinline__ void inv(uint32_t* x, int logn, int cnt0, int cnt1, const NttTables& T) {
+  if (logn == LOG2_N_MAX)
+    inv_t<LOG2_N_MAX>(x, logn, cnt0, cnt1, T);
+  else
+    inv_t<0>(x, logn, cnt0, cnt1, T);
 }
 
 }  // namespace ntt_detail
