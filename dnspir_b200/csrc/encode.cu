@@ -61,11 +61,26 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
   const uint32_t u0 = blockIdx.x * U;
   const uint32_t n2 = 1u << logn2;
   const uint32_t N = g.n;
-  for (uint32_t b = threadIdx.x; b < (uint32_t)U * n2; b += blockDim.x) {
-    const uint32_t t = b / U, uu = b % U;
-    uint32_t v = 0;
-    if (t < l_in) v = A[((size_t)t * nl + k) * N + u0 + uu];
-    sm[uu * n2 + t] = v;
+  if (U == 8) {
+    // one thread per t: the 8 slots are one 32-byte sector, and a warp's
+    // stores to each slot's row hit 32 consecutive banks
+    for (uint32_t t = threadIdx.x; t < n2; t += blockDim.x) {
+      uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+      if (t < l_in) {
+        const uint4* src = reinterpret_cast<const uint4*>(A + ((size_t)t * nl + k) * N + u0);
+        lo = __ldg(src);
+        hi = __ldg(src + 1);
+      }
+      sm[0 * n2 + t] = lo.x, sm[1 * n2 + t] = lo.y, sm[2 * n2 + t] = lo.z, sm[3 * n2 + t] = lo.w;
+      sm[4 * n2 + t] = hi.x, sm[5 * n2 + t] = hi.y, sm[6 * n2 + t] = hi.z, sm[7 * n2 + t] = hi.w;
+    }
+  } else {
+    for (uint32_t b = threadIdx.x; b < (uint32_t)U * n2; b += blockDim.x) {
+      const uint32_t t = b / U, uu = b % U;
+      uint32_t v = 0;
+      if (t < l_in) v = A[((size_t)t * nl + k) * N + u0 + uu];
+      sm[uu * n2 + t] = v;
+    }
   }
   __syncthreads();
   ntt_fwd_smem(sm, logn2, U, T, 0);

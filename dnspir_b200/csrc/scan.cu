@@ -181,11 +181,14 @@ __global__ void primary_epilogue_kernel(const uint32_t* __restrict__ fin, int ns
   const int s = blockIdx.x, l0 = blockIdx.y * 2, b = blockIdx.z;
   const int logn = g.log2n;
   const uint32_t N = g.n;
-  for (uint32_t x = threadIdx.x; x < 4 * N; x += blockDim.x) {
-    const uint32_t poly = x >> logn, k = x & (N - 1);
-    const int p = poly >> 1, ll = poly & 1;
-    sm[(poly << logn) + brv(k, logn)] =
-        fin[((((size_t)b * nshards + s) * 2 + p) * N + __ldg(uof + k)) * SIMD + l0 + ll];
+  // position x of factor p holds natural slot brv(x) of both lanes (one 8-byte
+  // load per pair; iterating over positions keeps the stores conflict-free)
+  for (uint32_t x = threadIdx.x; x < 2 * N; x += blockDim.x) {
+    const uint32_t p = x >> logn, xx = x & (N - 1);
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(
+        fin + ((((size_t)b * nshards + s) * 2 + p) * N + __ldg(uof + brv(xx, logn))) * SIMD + l0));
+    sm[((2 * p) << logn) + xx] = v.x;
+    sm[((2 * p + 1) << logn) + xx] = v.y;
   }
   __syncthreads();
   ntt_inv_smem2(sm, logn, 2, 2, T);
