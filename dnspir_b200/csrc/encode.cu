@@ -45,10 +45,8 @@ __global__ void encode_cols_kernel(const uint16_t* __restrict__ in, uint32_t* __
   for (uint32_t b = threadIdx.x; b < (uint32_t)cnt * n; b += blockDim.x) sm[b] = in[(size_t)first * n + b];
   __syncthreads();
   ntt_fwd_smem(sm, log2n, cnt, T, 0);
-  for (uint32_t b = threadIdx.x; b < (uint32_t)cnt * n; b += blockDim.x) {
-    const uint32_t poly = b >> log2n, u = b & (n - 1);
-    A[(size_t)(first + poly) * n + u] = sm[(poly << log2n) + brv(u, log2n)];
-  }
+  // transform-position order: position x holds slot brv(x)
+  for (uint32_t b = threadIdx.x; b < (uint32_t)cnt * n; b += blockDim.x) A[(size_t)first * n + b] = sm[b];
 }
 
 // One block: U consecutive slots u of one lane.  Transforms the length-l
@@ -58,7 +56,7 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
                                    NttTables T) {
   extern __shared__ uint32_t sm[];
   const int k = blockIdx.y;
-  const uint32_t u0 = blockIdx.x * U;
+  const uint32_t x0 = blockIdx.x * U;  // first transform position of the block
   const uint32_t n2 = 1u << logn2;
   const uint32_t N = g.n;
   if (U == 8) {
@@ -67,7 +65,7 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
     for (uint32_t t = threadIdx.x; t < n2; t += blockDim.x) {
       uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
       if (t < l_in) {
-        const uint4* src = reinterpret_cast<const uint4*>(A + ((size_t)t * nl + k) * N + u0);
+        const uint4* src = reinterpret_cast<const uint4*>(A + ((size_t)t * nl + k) * N + x0);
         lo = __ldg(src);
         hi = __ldg(src + 1);
       }
@@ -78,7 +76,7 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
     for (uint32_t b = threadIdx.x; b < (uint32_t)U * n2; b += blockDim.x) {
       const uint32_t t = b / U, uu = b % U;
       uint32_t v = 0;
-      if (t < l_in) v = A[((size_t)t * nl + k) * N + u0 + uu];
+      if (t < l_in) v = A[((size_t)t * nl + k) * N + x0 + uu];
       sm[uu * n2 + t] = v;
     }
   }
@@ -90,11 +88,13 @@ __global__ void encode_rows_kernel(const uint32_t* __restrict__ A, uint32_t* __r
     const uint32_t uu = b % U;
     const uint32_t r = (b / U) % g.L;
     const uint32_t h = b / (U * g.L);
-    const uint32_t u = u0 + uu;
+    // A and Ahat are in transform-position order: position x holds slot brv(x)
+    const uint32_t x = x0 + uu;
+    const uint32_t u = brv(x, g.log2n);
     const uint32_t g5 = ((2 * u + 1) * pow5[r]) & mask;
     // slot s of W holds V(zeta^(-qbp (2s+1))): main needs exponent (2u+1) qbp 5^r
     const uint32_t s = h == 0 ? ((mask + 1 - g5) & mask) >> 1 : g5 >> 1;
-    Ahat[(((size_t)h * g.L + r) * nl + k) * N + u] = sm[uu * n2 + brv(s, logn2)];
+    Ahat[(((size_t)h * g.L + r) * nl + k) * N + x] = sm[uu * n2 + brv(s, logn2)];
   }
 }
 
@@ -113,9 +113,10 @@ __global__ void encode_lift_kernel(const uint32_t* __restrict__ Ahat, uint32_t* 
   const int logn = g.log2n;
   uint32_t* x1 = sm;
   uint32_t* x2 = sm + nlg * N;
+  // Ahat rows are in transform-position order, the inverse transform's input order
   for (uint32_t b = threadIdx.x; b < (uint32_t)nlg * N; b += blockDim.x) {
-    const uint32_t kk = b >> logn, u = b & (N - 1);
-    x1[(kk << logn) + brv(u, logn)] = Ahat[(((size_t)h * g.L + r) * nl + lane0 + kk) * N + u];
+    const uint32_t kk = b >> logn;
+    x1[b] = Ahat[(((size_t)h * g.L + r) * nl + lane0 + kk) * N + (b & (N - 1))];
   }
   __syncthreads();
   ntt_inv_smem(x1, logn, nlg, T, 0);

@@ -41,10 +41,11 @@ __host__ __device__ __forceinline__ size_t slab_off(const Group& g, int p, int h
 __host__ __device__ __forceinline__ size_t slab_words(const Group& g) { return (size_t)2 * g.H * g.L * 3 * g.n * SIMD; }
 
 // ---- DB encoding (set_transformed_entries, base_pir.rs:662-772)
-// in: coefficients [t < l_in][lane < nl][n < N] (< t); A: [t][lane][u] (q1, natural slots)
+// in: coefficients [t < l_in][lane < nl][n < N] (< t); A: [t][lane][x] (q1, transform
+// position x = slot brv(x))
 void launch_encode_cols(const uint16_t* in, uint32_t* A, const Group& g, uint32_t l_in, int nl, const NttTables& T,
                         cudaStream_t st);
-// A -> Ahat[h][r][lane][u] (q1, natural slots): evaluations of column polys at the Galois orbit
+// A -> Ahat[h][r][lane][x] (q1, position x = slot brv(x)): evaluations of column polys at the Galois orbit
 void launch_encode_rows(const uint32_t* A, uint32_t* Ahat, const Group& g, uint32_t l_in, int nl, const NttTables& T,
                         cudaStream_t st);
 // Ahat -> transformed entries.  frame 0: scan layout in `slab` (nl == 8);
