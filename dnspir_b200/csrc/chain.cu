@@ -483,6 +483,235 @@ __device__ __forceinline__ void secondary_body(const ChainArgs& a, int h, int q,
   cluster.sync();  // keep this block's shared memory alive until the peer's last read
 }
 
+// ---- secondary chain without a cluster: one block carries one part at half h
+// in BOTH factors.  Every transform pass handles the two factors' vectors
+// (each with its own twiddles and prime), the high digit reads both inverse
+// transforms from this block's shared memory (no cluster barrier, no remote
+// reads), and each barrier covers twice the work of the clustered form.
+// Shared memory (u32 words): twiddles FW FWQ IW IWQ of each factor (8N), per
+// factor TC[2] D[2] B[2] H (7N): 22N = 176 KiB at N = 2048, one block per SM.
+constexpr int SEC_DUAL_WORDS = 8 + 2 * SEC_PART_WORDS;  // x N
+
+template <int LOGN>
+__device__ __forceinline__ void fwd_dual(uint32_t* x0, uint32_t* x1, int logn_rt, const uint32_t* const* tw,
+                                         const uint32_t* const* twq, uint32_t p0, uint32_t p1) {
+  const int logn = LOGN ? LOGN : logn_rt;
+  const int N = 1 << logn;
+  uint32_t* xs[2] = {x0, x1};
+  const uint32_t ps[2] = {p0, p1};
+  int s = 0;
+#pragma unroll
+  for (; s + 1 < logn; s += 2) {
+    const int logt2 = logn - s - 2;
+    const int t2 = 1 << logt2, t = 2 * t2, m = 1 << s;
+    for (int g = threadIdx.x; g < N / 4; g += CT) {
+      const int blk = g >> logt2, r = g & (t2 - 1);
+      const int j = (blk << (logt2 + 2)) + r;
+      uint32_t v[2][4];
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        const uint32_t* x = xs[l];
+        v[l][0] = x[j], v[l][1] = x[j + t2], v[l][2] = x[j + t], v[l][3] = x[j + t + t2];
+      }
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        const uint32_t w = tw[l][m + blk], wq = twq[l][m + blk];
+        ct_bf(v[l][0], v[l][2], w, wq, ps[l]);
+        ct_bf(v[l][1], v[l][3], w, wq, ps[l]);
+        ct_bf(v[l][0], v[l][1], tw[l][2 * m + 2 * blk], twq[l][2 * m + 2 * blk], ps[l]);
+        ct_bf(v[l][2], v[l][3], tw[l][2 * m + 2 * blk + 1], twq[l][2 * m + 2 * blk + 1], ps[l]);
+      }
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        uint32_t* x = xs[l];
+        x[j] = v[l][0], x[j + t2] = v[l][1], x[j + t] = v[l][2], x[j + t + t2] = v[l][3];
+      }
+    }
+    __syncthreads();
+  }
+  if (s < logn) {  // last stage, t = 1
+    for (int b = threadIdx.x; b < N / 2; b += CT) {
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        uint32_t* x = xs[l];
+        uint32_t u = x[2 * b], v = x[2 * b + 1];
+        ct_bf(u, v, tw[l][N / 2 + b], twq[l][N / 2 + b], ps[l]);
+        x[2 * b] = red2p(red2p(u, 2 * ps[l]), ps[l]);
+        x[2 * b + 1] = red2p(red2p(v, 2 * ps[l]), ps[l]);
+      }
+    }
+  } else {
+    for (int b = threadIdx.x; b < N; b += CT)
+#pragma unroll
+      for (int l = 0; l < 2; l++) xs[l][b] = red2p(red2p(xs[l][b], 2 * ps[l]), ps[l]);
+  }
+  __syncthreads();
+}
+
+template <int LOGN>
+__device__ __forceinline__ void inv_dual(uint32_t* x0, uint32_t* x1, int logn_rt, const uint32_t* const* tw,
+                                         const uint32_t* const* twq, uint32_t p0, uint32_t p1) {
+  const int logn = LOGN ? LOGN : logn_rt;
+  const int N = 1 << logn;
+  uint32_t* xs[2] = {x0, x1};
+  const uint32_t ps[2] = {p0, p1};
+  int s = 0;
+#pragma unroll
+  for (; s + 1 < logn; s += 2) {
+    const int t = 1 << s;
+    const int h0 = N >> (s + 1), h1 = N >> (s + 2);
+    for (int g = threadIdx.x; g < N / 4; g += CT) {
+      const int blk = g >> s, r = g & (t - 1);
+      const int j = (blk << (s + 2)) + r;
+      uint32_t v[2][4];
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        const uint32_t* x = xs[l];
+        v[l][0] = x[j], v[l][1] = x[j + t], v[l][2] = x[j + 2 * t], v[l][3] = x[j + 3 * t];
+      }
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        gs_bf(v[l][0], v[l][1], tw[l][h0 + 2 * blk], twq[l][h0 + 2 * blk], ps[l]);
+        gs_bf(v[l][2], v[l][3], tw[l][h0 + 2 * blk + 1], twq[l][h0 + 2 * blk + 1], ps[l]);
+        const uint32_t w = tw[l][h1 + blk], wq = twq[l][h1 + blk];
+        gs_bf(v[l][0], v[l][2], w, wq, ps[l]);
+        gs_bf(v[l][1], v[l][3], w, wq, ps[l]);
+      }
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        uint32_t* x = xs[l];
+        x[j] = v[l][0], x[j + t] = v[l][1], x[j + 2 * t] = v[l][2], x[j + 3 * t] = v[l][3];
+      }
+    }
+    __syncthreads();
+  }
+  if (s < logn) {  // last stage, t = N/2
+    for (int j = threadIdx.x; j < N / 2; j += CT) {
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        uint32_t* x = xs[l];
+        uint32_t u = x[j], v = x[j + N / 2];
+        gs_bf(u, v, tw[l][1], twq[l][1], ps[l]);
+        x[j] = u;
+        x[j + N / 2] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int LOGN>
+__device__ __forceinline__ void secondary_dual_body(const ChainArgs& a, int h, int q, int part, uint32_t* sm) {
+  const int logn = LOGN ? LOGN : a.g.log2n;
+  const int N = 1 << logn;
+  const uint32_t pr0 = a.cp[0].p, pr1 = a.cp[1].p;
+  const uint32_t* tws[2] = {sm, sm + 4 * N};
+  const uint32_t* twqs[2] = {sm + N, sm + 5 * N};
+  const uint32_t* itws[2] = {sm + 2 * N, sm + 6 * N};
+  const uint32_t* itwqs[2] = {sm + 3 * N, sm + 7 * N};
+  uint32_t* F0 = sm + 8 * N;  // factor blocks: TC[2] at 0, N; D[2] at 2N, 3N; B[2] at 4N, 5N; H at 6N
+  const int FS = SEC_PART_WORDS * N;
+  const int oTC = 0, oD = 2 * N, oB = 4 * N, oH = 6 * N;
+  const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
+  constexpr int PER = N_MAX / CT;
+  uint32_t kc[2][6][PER], dst[PER];
+#pragma unroll
+  for (int c = 0; c < PER; c++) {
+    const int pos = threadIdx.x + c * CT;
+    if (pos < N) {
+#pragma unroll
+      for (int p = 0; p < 2; p++) {
+        const ChainPrime& cp = a.cp[p];
+        const size_t o = (size_t)p * N + pos;
+        kc[p][0][c] = mont_reduce((uint64_t)a.gka[o] * cp.r2, cp.p, cp.pinv);
+        kc[p][1][c] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
+        kc[p][2][c] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+        kc[p][3][c] = mont_reduce((uint64_t)qq[o] * cp.r2, cp.p, cp.pinv);
+        kc[p][4][c] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
+        kc[p][5][c] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+      }
+      dst[c] = __ldg(a.galb + pos);
+    }
+  }
+  for (int b = threadIdx.x; b < N; b += CT) {
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      sm[4 * p * N + b] = a.T.fw[p][b];
+      sm[(4 * p + 1) * N + b] = a.T.fwq[p][b];
+      sm[(4 * p + 2) * N + b] = a.T.iw[p][b];
+      sm[(4 * p + 3) * N + b] = a.T.iwq[p][b];
+      F0[p * FS + oTC + b] = 0;
+      F0[p * FS + oD + b] = 0;
+      F0[p * FS + oB + b] = 0;
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = 0; i < a.g.L; i++) {
+    const int cur = (int)(i & 1) * N, nxt = N - cur;
+    uint32_t e[2][PER];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const uint32_t* Ei = a.E + ((((size_t)p * a.g.H + h) * a.g.L + i) * a.nl + (size_t)q * CTXT_PARTS + part) * N;
+#pragma unroll
+      for (int c = 0; c < PER; c++) {
+        const int pos = threadIdx.x + c * CT;
+        e[p][c] = pos < N ? __ldg(Ei + pos) : 0;
+      }
+    }
+    inv_dual<LOGN>(F0 + oD + cur, F0 + FS + oD + cur, logn, itws, itwqs, pr0, pr1);
+    for (int b = threadIdx.x; b < N; b += CT) {
+      const int32_t hd = high_digit(F0[oD + cur + b], F0[FS + oD + cur + b], a.cp[0], a.cp[1]);
+      F0[oH + b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr0) : (uint32_t)hd;
+      F0[FS + oH + b] = hd < 0 ? (uint32_t)(hd + (int32_t)pr1) : (uint32_t)hd;
+    }
+    __syncthreads();
+    fwd_dual<LOGN>(F0 + oH, F0 + FS + oH, logn, tws, twqs, pr0, pr1);
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+      const int pos = threadIdx.x + c * CT;
+      if (pos < N) {
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+          const ChainPrime& cp = a.cp[p];
+          uint32_t* P = F0 + p * FS;
+          const uint32_t n1 = P[oH + pos];
+          const uint32_t n0 = sub_mod(P[oTC + cur + pos], mont_reduce((uint64_t)n1 * cp.c26, cp.p, cp.pinv), cp.p);
+          const uint32_t an = mont_reduce(
+              (uint64_t)n0 * kc[p][0][c] + (uint64_t)n1 * kc[p][1][c] + (uint64_t)e[p][c] * kc[p][2][c], cp.p,
+              cp.pinv);
+          const uint32_t bn = mont_reduce(((uint64_t)P[oB + cur + pos] << 32) + (uint64_t)n0 * kc[p][3][c] +
+                                              (uint64_t)n1 * kc[p][4][c] + (uint64_t)e[p][c] * kc[p][5][c],
+                                          cp.p, cp.pinv);
+          P[oTC + nxt + dst[c]] = an;
+          P[oD + nxt + dst[c]] = an;
+          P[oB + nxt + dst[c]] = bn;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int fin = (int)(a.g.L & 1) * N;
+  uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + part) * 2) * 2 * N;
+#pragma unroll
+  for (int c = 0; c < PER; c++) {
+    const int pos = threadIdx.x + c * CT;
+    if (pos < N) {
+#pragma unroll
+      for (int p = 0; p < 2; p++) {
+        o[(size_t)p * N + pos] = F0[p * FS + oTC + fin + dst[c]];
+        o[2 * (size_t)N + (size_t)p * N + pos] = F0[p * FS + oB + fin + dst[c]];
+      }
+    }
+  }
+}
+
+// grid: x = part * H + half, y = query (no cluster)
+template <int LOGN>
+__global__ void __launch_bounds__(CT, 1) secondary_dual_kernel(ChainArgs a) {
+  extern __shared__ uint32_t sm[];
+  secondary_dual_body<LOGN>(a, blockIdx.x % a.g.H, blockIdx.y, blockIdx.x / a.g.H, sm);
+}
+
 // grid: x = factor (cluster of 2), y = (part group) * H + half, z = query
 template <int LN, int LOGN>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CT) secondary_chain_kernel(ChainArgs a) {
@@ -610,14 +839,15 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   a.qv_stride = qv_stride;
   a.nl = nq * CTXT_PARTS;
   a.out = out;
-  // one part per block (80 KiB: two blocks per SM, or one beside a scan
-  // block) unless the chunk's blocks exceed two per SM; three parts per
-  // block beyond that
+  // one part and factor per block in 2-block clusters (88 KiB; for a few
+  // queries: the chains run on many SMs, and a block fits beside a scan block)
+  // while the chunk needs at most one block per SM; beyond that one block per
+  // part carrying both factors (no cluster barrier, twice the work per barrier)
   int sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool full = g.log2n == LOG2_N_MAX;
-  if ((long)nq * CTXT_PARTS * g.H * 2 <= 2 * sms) {
+  if ((long)nq * CTXT_PARTS * g.H * 2 <= sms) {
     const size_t smem = chain_smem(g, 1);
     const dim3 grid(2, CTXT_PARTS * g.H, nq);
     if (full) {
@@ -628,14 +858,15 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
       secondary_chain_kernel<1, 0><<<grid, CT, smem, st>>>(a);
     }
   } else {
-    const size_t smem = chain_smem(g, CTXT_PARTS);
-    const dim3 grid(2, g.H, nq);
+    // larger chunks: one block per part and half carrying both factors
+    const size_t smem = (size_t)SEC_DUAL_WORDS * g.n * 4;
+    const dim3 grid(CTXT_PARTS * g.H, nq);
     if (full) {
-      set_smem(secondary_chain_kernel<CTXT_PARTS, LOG2_N_MAX>, smem);
-      secondary_chain_kernel<CTXT_PARTS, LOG2_N_MAX><<<grid, CT, smem, st>>>(a);
+      set_smem(secondary_dual_kernel<LOG2_N_MAX>, smem);
+      secondary_dual_kernel<LOG2_N_MAX><<<grid, CT, smem, st>>>(a);
     } else {
-      set_smem(secondary_chain_kernel<CTXT_PARTS, 0>, smem);
-      secondary_chain_kernel<CTXT_PARTS, 0><<<grid, CT, smem, st>>>(a);
+      set_smem(secondary_dual_kernel<0>, smem);
+      secondary_dual_kernel<0><<<grid, CT, smem, st>>>(a);
     }
   }
 }
