@@ -349,10 +349,9 @@ __device__ __forceinline__ void primary_body(const ChainArgs& a, int h, int lane
 
 // Secondary chain: LN of the three parts of one query's secondary ciphertext
 // at half h in one block (factor p = rank in the cluster), parts part0 ..
-// part0 + LN - 1.  With LN = 3 each transform pass and cluster barrier serves
-// three vectors (throughput: one wave holds SMs / (2 H) queries); with LN = 1
-// the block needs 128 KiB and shares an SM with a scan block (latency: the
-// chains of a few queries overlap the next scan).  The key constants gk_a0,
+// part0 + LN - 1 (the library launches LN = 1: the block then needs 88 KiB and
+// shares an SM with a scan block, so the chains of a few queries overlap the
+// next scan; larger chunks use secondary_dual_kernel below).  The key constants gk_a0,
 // gk_a1, qry_a, gk_b0, gk_b1, qry_b (Montgomery form) and the sigma_5
 // destinations of a thread's positions live in its registers.  Each step's
 // pointwise stage writes the next step's sigma_5-permuted a and b straight
