@@ -362,6 +362,7 @@ int dnspir_fleet_set_engine(dnspir_fleet* f, int engine) {
   f->batch = 1;
   f->tuned.clear();
   f->tuned_cc.clear();
+  f->tuned_serial.clear();
   return DNSPIR_OK;
 }
 
@@ -494,11 +495,32 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
       best_i = i;
     }
   }
+  // schedule: the best shape again with each group's primary phase waiting for
+  // the previous group's secondary phase; keep whichever is faster
+  bool serial = false;
+  if (rc == DNSPIR_OK && best_i >= 0) {
+    f->tuned[nb] = best_i;
+    f->tuned_serial[nb] = 1;
+    rc = dnspir_fleet_process_queries(f, ptrs.data(), lens.data(), (uint32_t)(nb * groups), r.as<uint8_t>(), RB,
+                                      nullptr, 1);
+    if (rc == DNSPIR_OK) {
+      std::lock_guard<std::mutex> lk(f->mu);
+      float t = 0;
+      if (cudaEventElapsedTime(&t, f->tev[6], f->tev[17]) == cudaSuccess && t / 2 < best) {
+        serial = true;
+        best = t / 2;
+        if (ms_per_shape) ms_per_shape[best_i] = best;
+      }
+      cudaGetLastError();
+    }
+  }
   f->batch = old_batch;
   f->tuned = old_tuned;
+  f->tuned_serial.erase(nb);
   if (rc != DNSPIR_OK) return rc;
   if (best_i < 0) return fail(DNSPIR_ERR_CUDA, "no tile shape ran");
   f->tuned[nb] = best_i;
+  f->tuned_serial[nb] = serial ? 1 : 0;
   if (chosen) *chosen = best_i;
   return DNSPIR_OK;
 }
@@ -694,6 +716,11 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
     cudaEvent_t* t = nullptr;
     CKR(group_events(f, gi, &t));
     CKR(slot_acquire(f, s));
+    // schedule: unless this group size overlaps, its primary phase waits for
+    // the previous group's secondary phase (the two phases then do not share SMs)
+    auto so = f->tuned_serial.find(nb);
+    if (so != f->tuned_serial.end() && so->second && f->slot[(gi & 1) ^ 1].sec_pending)
+      CK(cudaStreamWaitEvent(f->st, f->slot[(gi & 1) ^ 1].sec_done, 0));
     CKR(fleet_slot_workspace(f, s, Bk, nb, (size_t)nb * want));
     // host staging of the slot may still feed the copies of the group two back
     if (s.prim_recorded) CK(cudaEventSynchronize(s.prim_done));

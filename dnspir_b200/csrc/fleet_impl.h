@@ -54,6 +54,7 @@ struct dnspir_fleet {
   dnspir::DBuf qb, err_word, tmp_lane;        // tensor engine: query operand, wait-error word, preprocessing scratch
   std::map<int, int> tuned;                   // tensor engine: group size -> tile shape index
   std::map<int, int> tuned_cc;                // CUDA-core engine: group size -> queries per block
+  std::map<int, int> tuned_serial;            // group size -> 1: primary waits for the previous secondary
   std::vector<cudaEvent_t> tev;               // 6 timing events per group of the last call
   std::vector<int> q_group;                   // per query of the last call: its group, or -1
   std::mutex mu;

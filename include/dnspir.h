@@ -142,7 +142,9 @@ int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, ui
  * replies; zero query bytes, two timed groups after one warm-up) instead of
  * the scan alone: the shape that maximises responses/s when the secondary
  * phase of one group overlaps the scan of the next.  ms_per_shape receives
- * milliseconds per group. */
+ * milliseconds per group.  The schedule is tuned too: the best shape is timed
+ * again with each group's primary phase waiting for the previous group's
+ * secondary phase, and that schedule is kept for the group size when faster. */
 int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
 /* CUDA-core engine: time the scan of a group of `batch` queries (a power of two
  * up to 256, one launch) with 1, 2, 4, 8 and 16 queries per block and keep the
