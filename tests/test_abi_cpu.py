@@ -77,6 +77,28 @@ def test_no_cpu_fallback():
     with pytest.raises(dp.DnspirError) as e:
         dp.PIRDatabase(8, 256)
     assert e.value.code == 4
+    with pytest.raises(dp.DnspirError) as e:
+        dp.Server(max_sessions=4)
+    assert e.value.code == 4
+
+
+def test_null_handles_are_rejected():
+    # every entry point checks its handle instead of crashing
+    import ctypes
+    L = dp.lib()
+    t = ctypes.c_uint64()
+    done = ctypes.c_int()
+    assert L.dnspir_server_submit(None, 0, -1, b"x", 1, ctypes.byref(t)) == 6
+    assert L.dnspir_server_poll(None, 1, None, 0, ctypes.byref(done)) == 6
+    assert L.dnspir_server_start(None, 1) == 6
+    assert L.dnspir_server_set_batching(None, 0, 1, 0) == 6
+    assert L.dnspir_fleet_set_batch(None, 1) == 6
+    assert L.dnspir_fleet_set_engine(None, 1) == 6
+    assert L.dnspir_fleet_tune(None, 1, None, None) == 6
+    assert L.dnspir_fleet_tune_pipeline(None, 1, None, None) == 6
+    assert L.dnspir_fleet_tune_cuda_cores(None, 1, None, None) == 6
+    assert L.dnspir_fleet_set_tile(None, 1, 0) == 6
+    assert L.dnspir_server_destroy(None) == 0 and L.dnspir_fleet_destroy(None) == 0
 
 
 @pytest.mark.parametrize("entries,i,j", [(32768, 0, 0), (32768, 8191, 3), (1 << 20, 12345, 63), (1 << 22, 16383, 255)])
