@@ -565,7 +565,7 @@ def main():
     achieved = algo_bytes / (scan_avg * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     kname = "tscan_kernel" if args.engine == "tensor" else "scan_batch_kernel"
-    traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_plain_2p22.md")
+    traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_batch_2p22.md")
     value = whole_job_rate(args.steps, world, total_ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
