@@ -200,8 +200,6 @@ int fleet_primary_kernels(dnspir_fleet* f, QSlot& s, int nb, int Bk, const uint3
   if (scan0) CK(cudaEventRecord(scan0, f->st));
   CKR(launch_scan(f, s, nb, Bk));
   if (scan1) CK(cudaEventRecord(scan1, f->st));
-  launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
-                          s.sec_in.as<uint16_t>(), f->sec_chunk, g1, slot_maps(f->ctx, g1.log2n), f->ctx->T, f->st);
   CK(cudaGetLastError());
   return DNSPIR_OK;
 }
@@ -212,6 +210,11 @@ int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_de
   const size_t n = g2.n;
   cudaStream_t st = f->sec;
   const uint32_t l_in = f->S * SIMD;
+  // the primary epilogue (scan output -> secondary entries) runs here, on the
+  // secondary stream, so that the next group's scan does not wait for it; it
+  // reads and writes only this slot's buffers
+  launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
+                          s.sec_in.as<uint16_t>(), f->sec_chunk, f->g1, slot_maps(f->ctx, f->g1.log2n), f->ctx->T, st);
   const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
   const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
   for (int c0 = 0; c0 < nb; c0 += f->sec_chunk) {

@@ -76,11 +76,11 @@ int fleet_slot_workspace(dnspir_fleet* f, QSlot& s, int Bk, int nb, size_t qbyte
 // Secondary workspace for groups of up to nb queries.
 int fleet_secondary_workspace(dnspir_fleet* f, int nb);
 // Primary kernels of a group on f->st: decode (bytes and descriptors already
-// in s.qbytes / s.qdesc), scan, epilogue.  scan0/scan1: optional events
-// around the scan.
+// in s.qbytes / s.qdesc) and scan.  scan0/scan1: optional events around the
+// scan.
 int fleet_primary_kernels(dnspir_fleet* f, QSlot& s, int nb, int Bk, const uint32_t* sess_nat,
                           const uint32_t* sess_brv, cudaEvent_t scan0, cudaEvent_t scan1);
-// Secondary kernels of a group on f->sec: encode, chains, replies (bytes at
+// Secondary kernels of a group on f->sec: primary epilogue, encode, chains, replies (bytes at
 // reply_dev + q * reply_stride, or Z_q ciphertexts at reply_zq), and the copy
 // of nb reply bytes to host_reply when given.
 int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_dev, size_t reply_stride,
