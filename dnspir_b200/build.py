@@ -20,7 +20,7 @@ FLAGS = [
 def build(verbose=False, extra=()):
     srcs = [os.path.join(HERE, "csrc", s) for s in SRC]
     newest = max(os.path.getmtime(p) for p in srcs + [os.path.join(HERE, "csrc", h) for h in
-                                                   ("common.cuh", "ntt.cuh", "kernels.cuh", "host.h", "fleet_impl.h")] +
+                                                   ("common.cuh", "ntt.cuh", "ntt2048.cuh", "kernels.cuh", "host.h", "fleet_impl.h")] +
                  [os.path.join(ROOT, "include", "dnspir.h")])
     if os.path.exists(OUT) and os.path.getmtime(OUT) >= newest and not extra:
         return OUT

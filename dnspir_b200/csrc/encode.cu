@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "ntt2048.cuh"
 
 namespace dnspir {
 
@@ -157,6 +158,131 @@ __global__ void encode_lift_kernel(const uint32_t* __restrict__ Ahat, uint32_t* 
   }
 }
 
+// ---- N = 2048: the same three steps on the register transforms of
+// ntt2048.cuh (padded shared layout, 512 threads, 16-byte global accesses).
+constexpr int NT2K = 512;
+constexpr uint32_t LIFT_M = TPLAIN << 15;  // a multiple of t above q1 / 2
+
+__global__ void __launch_bounds__(NT2K) encode_cols2k_kernel(const uint16_t* __restrict__ in,
+                                                             uint32_t* __restrict__ A, uint32_t total, int ppc,
+                                                             NttTables T) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  using namespace n2k;
+  const uint32_t first = blockIdx.x * ppc;
+  const int cnt = min((uint32_t)ppc, total - first);
+  for (int b = threadIdx.x; b < cnt * (N / 4); b += NT2K) {
+    const int kk = b >> 9, q = b & (N / 4 - 1);
+    const uint2 w = __ldg(reinterpret_cast<const uint2*>(in + ((size_t)first + kk) * N) + q);
+    *reinterpret_cast<uint4*>(sm + kk * PS + phys(4 * q)) =
+        make_uint4(w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16);
+  }
+  __syncthreads();
+  fwd<NT2K>(sm, cnt, 0, T);
+  // transform-position order: position x holds slot brv(x)
+  for (int b = threadIdx.x; b < cnt * (N / 4); b += NT2K) {
+    const int kk = b >> 9, q = b & (N / 4 - 1);
+    reinterpret_cast<uint4*>(A + ((size_t)first + kk) * N)[q] =
+        *reinterpret_cast<const uint4*>(sm + kk * PS + phys(4 * q));
+  }
+}
+
+// One block: 8 consecutive transform positions x0 .. x0 + 7 of one lane, the
+// length-2048 transform over t (qbp = 1), both halves' orbit values written.
+__global__ void __launch_bounds__(NT2K) encode_rows2k_kernel(const uint32_t* __restrict__ A,
+                                                             uint32_t* __restrict__ Ahat, Group g, uint32_t l_in,
+                                                             int nl, const uint32_t* __restrict__ pow5,
+                                                             NttTables T) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  using namespace n2k;
+  const int k = blockIdx.y;
+  const uint32_t x0 = blockIdx.x * 8;
+  for (uint32_t t = threadIdx.x; t < (uint32_t)N; t += NT2K) {
+    uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
+    if (t < l_in) {
+      const uint4* src = reinterpret_cast<const uint4*>(A + ((size_t)t * nl + k) * N + x0);
+      lo = __ldg(src);
+      hi = __ldg(src + 1);
+    }
+    const uint32_t o = phys(t);
+    sm[0 * PS + o] = lo.x, sm[1 * PS + o] = lo.y, sm[2 * PS + o] = lo.z, sm[3 * PS + o] = lo.w;
+    sm[4 * PS + o] = hi.x, sm[5 * PS + o] = hi.y, sm[6 * PS + o] = hi.z, sm[7 * PS + o] = hi.w;
+  }
+  __syncthreads();
+  fwd<NT2K>(sm, 8, 0, T);
+  constexpr uint32_t mask = 2 * N - 1;
+  const int uu = threadIdx.x & 7;
+  const uint32_t x = x0 + uu;
+  const uint32_t odd = 2 * brv11(x) + 1;  // A and Ahat are in transform-position order
+  const uint32_t* w = sm + uu * PS;
+  for (uint32_t r = threadIdx.x >> 3; r < g.L; r += NT2K / 8) {
+    // slot s of W holds V(zeta^(-(2s+1))): the main half needs exponent (2u+1) 5^r
+    const uint32_t g5 = (odd * __ldg(pow5 + r)) & mask;
+    Ahat[((size_t)r * nl + k) * N + x] = w[phys(brv11(((mask + 1 - g5) & mask) >> 1))];
+    if (g.H == 2) Ahat[(((size_t)g.L + r) * nl + k) * N + x] = w[phys(brv11(g5 >> 1))];
+  }
+}
+
+// Ends the inverse transform of the lift: coefficient v (mod q1, unscaled)
+// -> c = centred(v N^-1), y = centred((c l^-1) mod t), written as y mod q1 in
+// place and y mod q2 into polynomial cnt + poly.  (c l^-1) mod t is taken as
+// (u s) mod t with u = c + LIFT_M > 0 and a Shoup quotient for s = l^-1 mod t.
+struct LiftFin {
+  int cnt;
+  uint32_t s, sq;  // l^-1 mod t and floor(s 2^32 / t)
+  __device__ __forceinline__ void operator()(uint32_t* y, int, int, uint32_t (&v)[8], uint32_t p, uint32_t ni,
+                                             uint32_t niq) const {
+    using namespace n2k;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t c = red(lazy_mul(v[k], ni, niq, p), p);
+      const uint32_t u = c + (c > P1 / 2 ? LIFT_M - P1 : LIFT_M);
+      uint32_t m = u * s - __umulhi(u, sq) * TPLAIN;  // in [0, 2t)
+      m = m >= TPLAIN ? m - TPLAIN : m;
+      const bool neg = m > TPLAIN / 2;
+      y[k * Geo8<1>::STR] = neg ? m + (P1 - TPLAIN) : m;
+      y[cnt * PS + k * Geo8<1>::STR] = neg ? m + (P2 - TPLAIN) : m;
+    }
+  }
+};
+
+// One block: column r of half h for up to LIFT_LANES_CHAIN lanes, chain layout.
+__global__ void __launch_bounds__(NT2K) encode_lift2k_kernel(const uint32_t* __restrict__ Ahat,
+                                                             uint32_t* __restrict__ out, Group g, int nl,
+                                                             uint32_t scale, uint32_t scale_q,
+                                                             const uint32_t* __restrict__ pow5inv, NttTables T) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  using namespace n2k;
+  const uint32_t r = blockIdx.x, h = blockIdx.y;
+  const int lane0 = blockIdx.z * LIFT_LANES_CHAIN;
+  const int nlg = min(LIFT_LANES_CHAIN, nl - lane0);
+  for (int b = threadIdx.x; b < nlg * (N / 4); b += NT2K) {
+    const int kk = b >> 9, q = b & (N / 4 - 1);
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(Ahat + (((size_t)h * g.L + r) * nl + lane0 + kk) * N) + q);
+    *reinterpret_cast<uint4*>(sm + kk * PS + phys(4 * q)) = v;
+  }
+  __syncthreads();
+  inv<NT2K>(sm, nlg, 0, T, LiftFin{nlg, scale, scale_q});
+  fwd<NT2K>(sm, nlg, nlg, T);
+  // E_c[j] = E^_r[idx(5^-r (2j+1))] at bit-reversed position brv(j)
+  const uint32_t c = g.L - 1 - r;
+  const uint32_t pw = __ldg(pow5inv + r);
+  constexpr uint32_t mask = 2 * N - 1;
+  for (int q = threadIdx.x; q < N / 4; q += NT2K) {
+    uint32_t idx[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const uint32_t j = brv11(4 * q + m);
+      idx[m] = phys(brv11(((pw * (2 * j + 1)) & mask) >> 1));
+    }
+    for (int pk = 0; pk < 2 * nlg; pk++) {
+      const int pp = pk >= nlg, kk = pk - pp * nlg;
+      const uint32_t* s = sm + pk * PS;
+      reinterpret_cast<uint4*>(out + ((((size_t)pp * g.H + h) * g.L + c) * nl + lane0 + kk) * N)[q] =
+          make_uint4(s[idx[0]], s[idx[1]], s[idx[2]], s[idx[3]]);
+    }
+  }
+}
+
 __global__ void pack_bytes_kernel(const uint8_t* __restrict__ bytes, uint16_t* __restrict__ coeffs, size_t groups) {
   // pack_bytes_into_coeffs (dns/bucket.rs:289-303): 5 bytes -> 4 ten-bit coefficients
   const size_t gi = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -209,6 +335,13 @@ void launch_encode_cols(const uint16_t* in, uint32_t* A, const Group& g, uint32_
                         cudaStream_t st) {
   const uint32_t total = l_in * nl;
   if (!total) return;
+  if (g.log2n == 11) {
+    const int ppc = 4;
+    const size_t smem = (size_t)ppc * n2k::PS * 4;
+    set_smem(encode_cols2k_kernel, smem);
+    encode_cols2k_kernel<<<(total + ppc - 1) / ppc, NT2K, smem, st>>>(in, A, total, ppc, T);
+    return;
+  }
   const int ppc = g.n >= 1024 ? 4 : 8;
   const size_t smem = (size_t)ppc * g.n * 4;
   const uint32_t blocks = (total + ppc - 1) / ppc;
@@ -220,6 +353,12 @@ void launch_encode_rows(const uint32_t* A, uint32_t* Ahat, const Group& g, uint3
                         cudaStream_t st) {
   const int logn2 = g.log2n - __builtin_ctz(g.qbp);
   const uint32_t n2 = 1u << logn2;
+  if (g.log2n == 11 && logn2 == 11) {
+    const size_t smem = (size_t)8 * n2k::PS * 4;
+    set_smem(encode_rows2k_kernel, smem);
+    encode_rows2k_kernel<<<dim3(g.n / 8, nl), NT2K, smem, st>>>(A, Ahat, g, l_in, nl, pow_table(g.log2n, false), T);
+    return;
+  }
   int U = 8;
   while (U > 1 && (uint32_t)U > g.n) U >>= 1;
   const size_t smem = (size_t)U * n2 * 4;
@@ -233,6 +372,15 @@ void launch_encode_lift(const uint32_t* Ahat, uint32_t* out, const Group& g, int
   uint32_t linv = 1;
   for (uint32_t x = 1; x < TPLAIN; x++)
     if ((x * (g.l % TPLAIN)) % TPLAIN == 1) linv = x;
+  if (g.log2n == 11 && frame == 1) {
+    const uint32_t sq = (uint32_t)(((uint64_t)linv << 32) / TPLAIN);
+    const int nlg = nl < LIFT_LANES_CHAIN ? nl : LIFT_LANES_CHAIN;
+    const size_t smem = (size_t)2 * nlg * n2k::PS * 4;
+    dim3 grid(g.L, g.H, (nl + LIFT_LANES_CHAIN - 1) / LIFT_LANES_CHAIN);
+    set_smem(encode_lift2k_kernel, smem);
+    encode_lift2k_kernel<<<grid, NT2K, smem, st>>>(Ahat, out, g, nl, linv, sq, pow_table(g.log2n, true), T);
+    return;
+  }
   // frame 0 writes the 8 lanes of a slot together; frame 1 (chain layout)
   // takes fewer lanes per block so that three blocks fit on an SM
   const int lpb = frame == 0 ? 8 : LIFT_LANES_CHAIN;
