@@ -28,6 +28,7 @@
 #include <cstring>
 
 #include "kernels.cuh"
+#include "ntt2048.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -704,6 +705,153 @@ __device__ __forceinline__ void secondary_dual_body(const ChainArgs& a, int h, i
   }
 }
 
+// ---- N = 2048: one block per part and half carrying both factors, on the
+// register transforms of ntt2048.cuh.  The state a, b stays in natural
+// position order: instead of scattering the next step's sigma_5(a), sigma_5(b)
+// (which needs a second buffer of each), every step gathers them at its own
+// positions through the inverse of galb.  Thread t owns positions 4t .. 4t + 3
+// of both factors in the first inverse pass, the last forward pass and the
+// pointwise stage, so those run from registers; between the last inverse pass
+// and the first forward pass the two factors' threads of a butterfly group
+// swap their values once and both take the high digit.  Eight barriers a step.
+// Shared memory, padded polynomials of n2k::PS words: A[2] (a; also the
+// forward transform's work space), B[2] (b), D[2] (inverse work space).
+constexpr int SEC2K_WORDS = 6 * n2k::PS;
+
+__global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  using namespace n2k;
+  static_assert(CT == 512 && N_MAX == N, "one quad per thread and factor");
+  const int h = blockIdx.x % a.g.H, part = blockIdx.x / a.g.H, q = blockIdx.y;
+  uint32_t* const A = sm;
+  uint32_t* const B = sm + 2 * PS;
+  uint32_t* const D = sm + 4 * PS;
+  const int tid = threadIdx.x;
+  const int qb = (int)phys(4 * tid);  // this thread's quad
+  const uint32_t pr[2] = {a.cp[0].p, a.cp[1].p};
+  // sigma_5 sources of the quad (galb inverted through D), a = b = 0
+  for (int b = tid; b < N; b += CT) D[__ldg(a.galb + b)] = b;
+  for (int b = tid; b < 4 * PS; b += CT) sm[b] = 0;
+  __syncthreads();
+  uint32_t src[4];
+#pragma unroll
+  for (int m = 0; m < 4; m++) src[m] = phys(D[4 * tid + m]);
+  const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
+  uint32_t kc[2][6][4];
+#pragma unroll
+  for (int f = 0; f < 2; f++) {
+    const ChainPrime& cp = a.cp[f];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const size_t o = (size_t)f * N + 4 * tid + m;
+      kc[f][0][m] = mont_reduce((uint64_t)a.gka[o] * cp.r2, cp.p, cp.pinv);
+      kc[f][1][m] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
+      kc[f][2][m] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+      kc[f][3][m] = mont_reduce((uint64_t)qq[o] * cp.r2, cp.p, cp.pinv);
+      kc[f][4][m] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
+      kc[f][5][m] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+    }
+  }
+  __syncthreads();  // the table in D is overwritten by the first step
+  const size_t lane = (size_t)q * CTXT_PARTS + part;
+  for (uint32_t i = 0; i < a.g.L; i++) {
+    // entries of row i at the quad, consumed by the pointwise stage
+    uint4 e[2];
+#pragma unroll
+    for (int f = 0; f < 2; f++)
+      e[f] = __ldg(reinterpret_cast<const uint4*>(a.E + ((((size_t)f * a.g.H + h) * a.g.L + i) * a.nl + lane) * N) +
+                   tid);
+    // sigma_5(a) (the inverse transform's input and the kept t) and sigma_5(b)
+    uint32_t ta[2][4], tb[2][4];
+#pragma unroll
+    for (int f = 0; f < 2; f++)
+#pragma unroll
+      for (int m = 0; m < 4; m++) ta[f][m] = A[f * PS + src[m]], tb[f][m] = B[f * PS + src[m]];
+    // inverse stages 0-1 from registers
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const uint32_t* __restrict__ iw = a.T.iw[f];
+      const uint32_t* __restrict__ iwq = a.T.iwq[f];
+      uint4 v = make_uint4(ta[f][0], ta[f][1], ta[f][2], ta[f][3]);
+      gs(v.x, v.y, __ldg(iw + 1024 + 2 * tid), __ldg(iwq + 1024 + 2 * tid), pr[f]);
+      gs(v.z, v.w, __ldg(iw + 1024 + 2 * tid + 1), __ldg(iwq + 1024 + 2 * tid + 1), pr[f]);
+      const uint32_t w = __ldg(iw + 512 + tid), wq = __ldg(iwq + 512 + tid);
+      gs(v.x, v.z, w, wq, pr[f]);
+      gs(v.y, v.w, w, wq, pr[f]);
+      *reinterpret_cast<uint4*>(D + f * PS + qb) = v;
+    }
+    __syncthreads();
+    pass8<CT, 64, true>(D, 1, 1, a.T, (void*)nullptr);
+    pass8<CT, 8, true>(D, 1, 1, a.T, (void*)nullptr);
+    {
+      // last inverse pass (unscaled: N^-1 sits in the CRT constants), swap,
+      // high digit, first forward pass; factor f, group g, words g + 256 k
+      const int f = tid >> 8, g = tid & 255;
+      const int base = (int)phys(g);
+      constexpr int STR = Geo8<1>::STR;
+      uint32_t v[8];
+      uint32_t* y = D + f * PS + base;
+#pragma unroll
+      for (int k = 0; k < 8; k++) v[k] = y[k * STR];
+      inv8_bf(v, load_tw8(a.T.iw[f], a.T.iwq[f], 1, 0), pr[f]);
+#pragma unroll
+      for (int k = 0; k < 8; k++) y[k * STR] = v[k];
+      __syncthreads();
+      const uint32_t* z = D + (1 - f) * PS + base;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t o = z[k * STR];
+        const int32_t hd = f == 0 ? high_digit(v[k], o, a.cp[0], a.cp[1]) : high_digit(o, v[k], a.cp[0], a.cp[1]);
+        v[k] = hd < 0 ? (uint32_t)(hd + (int32_t)pr[f]) : (uint32_t)hd;
+      }
+      fwd8_bf(v, load_tw8(a.T.fw[f], a.T.fwq[f], 1, 0), pr[f]);
+      uint32_t* w = A + f * PS + base;
+#pragma unroll
+      for (int k = 0; k < 8; k++) w[k * STR] = v[k];
+      __syncthreads();
+    }
+    pass8<CT, 8, false>(A, 1, 1, a.T, (void*)nullptr);
+    pass8<CT, 64, false>(A, 1, 1, a.T, (void*)nullptr);
+    // forward stages 9-10 and the pointwise stage at the quad
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const ChainPrime& cp = a.cp[f];
+      const uint32_t p = pr[f];
+      const uint32_t* __restrict__ fw = a.T.fw[f];
+      const uint32_t* __restrict__ fwq = a.T.fwq[f];
+      uint4 v = *reinterpret_cast<const uint4*>(A + f * PS + qb);
+      const uint32_t w = __ldg(fw + 512 + tid), wq = __ldg(fwq + 512 + tid);
+      ct(v.x, v.z, w, wq, p);
+      ct(v.y, v.w, w, wq, p);
+      ct(v.x, v.y, __ldg(fw + 1024 + 2 * tid), __ldg(fwq + 1024 + 2 * tid), p);
+      ct(v.z, v.w, __ldg(fw + 1024 + 2 * tid + 1), __ldg(fwq + 1024 + 2 * tid + 1), p);
+      const uint32_t n1s[4] = {red(red(v.x, 2 * p), p), red(red(v.y, 2 * p), p), red(red(v.z, 2 * p), p),
+                               red(red(v.w, 2 * p), p)};
+      const uint32_t es[4] = {e[f].x, e[f].y, e[f].z, e[f].w};
+      uint32_t an[4], bn[4];
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const uint32_t n1 = n1s[m];
+        const uint32_t n0 = sub_mod(ta[f][m], mont_reduce((uint64_t)n1 * cp.c26, p, cp.pinv), p);
+        an[m] = mont_reduce((uint64_t)n0 * kc[f][0][m] + (uint64_t)n1 * kc[f][1][m] + (uint64_t)es[m] * kc[f][2][m], p,
+                            cp.pinv);
+        bn[m] = mont_reduce(((uint64_t)tb[f][m] << 32) + (uint64_t)n0 * kc[f][3][m] + (uint64_t)n1 * kc[f][4][m] +
+                                (uint64_t)es[m] * kc[f][5][m],
+                            p, cp.pinv);
+      }
+      *reinterpret_cast<uint4*>(A + f * PS + qb) = make_uint4(an[0], an[1], an[2], an[3]);
+      *reinterpret_cast<uint4*>(B + f * PS + qb) = make_uint4(bn[0], bn[1], bn[2], bn[3]);
+    }
+    __syncthreads();
+  }
+  uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + part) * 2) * 2 * N;
+#pragma unroll
+  for (int f = 0; f < 2; f++) {
+    reinterpret_cast<uint4*>(o + (size_t)f * N)[tid] = *reinterpret_cast<const uint4*>(A + f * PS + qb);
+    reinterpret_cast<uint4*>(o + 2 * (size_t)N + (size_t)f * N)[tid] = *reinterpret_cast<const uint4*>(B + f * PS + qb);
+  }
+}
+
 // grid: x = part * H + half, y = query (no cluster)
 template <int LOGN>
 __global__ void __launch_bounds__(CT, 1) secondary_dual_kernel(ChainArgs a) {
@@ -838,10 +986,11 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   a.qv_stride = qv_stride;
   a.nl = nq * CTXT_PARTS;
   a.out = out;
-  // one part and factor per block in 2-block clusters (88 KiB; for a few
-  // queries: the chains run on many SMs, and a block fits beside a scan block)
-  // while the chunk needs at most one block per SM; beyond that one block per
-  // part carrying both factors (no cluster barrier, twice the work per barrier)
+  // one part and factor per block in 2-block clusters (88 KiB, 64 registers;
+  // for a few queries: the chains run on many SMs, and a block fits beside a
+  // scan block) while the chunk needs at most one block per SM; beyond that one
+  // block per part carrying both factors (no cluster barrier, twice the work
+  // per barrier): at N = 2048 the register-transform kernel, else the generic one
   int sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -856,17 +1005,14 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
       set_smem(secondary_chain_kernel<1, 0>, smem);
       secondary_chain_kernel<1, 0><<<grid, CT, smem, st>>>(a);
     }
+  } else if (full) {
+    const size_t smem = (size_t)SEC2K_WORDS * 4;
+    set_smem(secondary_chain2k_kernel, smem);
+    secondary_chain2k_kernel<<<dim3(CTXT_PARTS * g.H, nq), CT, smem, st>>>(a);
   } else {
-    // larger chunks: one block per part and half carrying both factors
     const size_t smem = (size_t)SEC_DUAL_WORDS * g.n * 4;
-    const dim3 grid(CTXT_PARTS * g.H, nq);
-    if (full) {
-      set_smem(secondary_dual_kernel<LOG2_N_MAX>, smem);
-      secondary_dual_kernel<LOG2_N_MAX><<<grid, CT, smem, st>>>(a);
-    } else {
-      set_smem(secondary_dual_kernel<0>, smem);
-      secondary_dual_kernel<0><<<grid, CT, smem, st>>>(a);
-    }
+    set_smem(secondary_dual_kernel<0>, smem);
+    secondary_dual_kernel<0><<<dim3(CTXT_PARTS * g.H, nq), CT, smem, st>>>(a);
   }
 }
 

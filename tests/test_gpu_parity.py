@@ -244,3 +244,49 @@ def test_cuda_core_engine_large_groups(config1, batch):
             assert r == orc.process_query(refs, q), k
             i, j = (331 * k) % 8192, k % shards
             assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64))
+
+
+@pytest.fixture(scope="module")
+def full_secondary():
+    # the secondary database of 2^22 entries: the full group of order N = 2048
+    # (both halves, 1024 chain steps per half), here under a small primary
+    # group (l1 = 32, 256 shards on 2 distinct) so that the oracle answers in
+    # seconds
+    l1, l2, count, distinct = 32, 2048, 256, 2
+    data, refs, fleet = _fleets(11, l1, l2, count, distinct, 700)
+    return data, refs, fleet, l1, l2, count
+
+
+@pytest.mark.parametrize("batch,nq", [(1, 1), (2, 3)])
+def test_full_secondary_group_matches_oracle(full_secondary, batch, nq):
+    data, refs, fleet, l1, l2, count = full_secondary
+    rng = orc.Rng(bytes([6, batch]) + bytes(30))
+    picks = [(17, 200), (8 * l1 - 1, 255), (0, 0)][:nq]
+    qs = [orc.prepare_query(rng, i, j, l1, l2) for i, j in picks]
+    fleet.set_batch(batch)
+    try:
+        got = fleet.process_queries([q for q, _ in qs])
+    finally:
+        fleet.set_batch(1)
+    for (i, j), (q, seed), r in zip(picks, qs, got):
+        assert r == orc.process_query(refs, q), (i, j)
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), (i, j)
+
+
+def test_full_secondary_group_large_chunk(full_secondary):
+    # 16 queries: their secondary chains no longer fit one block per SM as
+    # 2-block clusters, so the one-block-per-part kernel runs; three replies
+    # are compared with the oracle byte for byte, all sixteen are decrypted
+    data, refs, fleet, l1, l2, count = full_secondary
+    rng = orc.Rng(bytes([7]) + bytes(31))
+    picks = [((37 * k + 5) % (8 * l1), (29 * k + 3) % count) for k in range(16)]
+    qs = [orc.prepare_query(rng, i, j, l1, l2) for i, j in picks]
+    fleet.set_batch(16)
+    try:
+        got = fleet.process_queries([q for q, _ in qs])
+    finally:
+        fleet.set_batch(1)
+    for k, ((i, j), (q, seed), r) in enumerate(zip(picks, qs, got)):
+        if k in (0, 7, 15):
+            assert r == orc.process_query(refs, q), k
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), k
