@@ -18,6 +18,7 @@
 // shard; blocks retire after their item so that the higher-priority secondary
 // stream can take SMs while a scan is running.
 #include "kernels.cuh"
+#include "ntt2048.cuh"
 
 namespace dnspir {
 namespace {
@@ -214,6 +215,68 @@ __global__ void primary_epilogue_kernel(const uint32_t* __restrict__ fin, int ns
   }
 }
 
+// ---- N = 2048: the same epilogue on the register transforms of
+// ntt2048.cuh.  Grid: x = shard, y = four lanes, z = query.  One 16-byte
+// gather per position and factor brings four lanes (half a 32-byte sector; the
+// other half is the neighbouring block's), the eight inverse transforms run
+// together, the CRT uses Shoup companions of its two constants and the 12-bit
+// switch an exact 64-bit rounding (v 2^13 + q < 2^64 for v < q).
+constexpr int EPI_NT = 512;
+
+__device__ __forceinline__ uint32_t ms_encode12(uint64_t v) {
+  // round(v 2^12 / q) = floor((v 2^13 + q) / 2q): a double estimate, then
+  // one exact correction (r <= 2^12, so r 2q < 2^64)
+  const uint64_t num = (v << (PRIM_B_BITS + 1)) + QQ;
+  int64_t r = (int64_t)floor((double)v * (double)(1u << PRIM_B_BITS) / (double)QQ + 0.5);
+  r = r < 0 ? 0 : r;
+  const uint64_t lo = (uint64_t)r * (2 * QQ);
+  if (num < lo) r--;
+  else if (num - lo >= 2 * QQ) r++;
+  return (uint32_t)r & ((1u << PRIM_B_BITS) - 1);
+}
+
+__global__ void __launch_bounds__(EPI_NT) primary_epilogue2k_kernel(
+    const uint32_t* __restrict__ fin, int nshards, const uint32_t* __restrict__ a_ms,
+    const int* __restrict__ distinct_of, uint16_t* __restrict__ sec_in, int nq, int chunk,
+    const uint32_t* __restrict__ uof, NttTables T, uint32_t k1, uint32_t k1q, uint32_t k2, uint32_t k2q) {
+  extern __shared__ __align__(16) uint32_t sm[];  // [q1 lanes l0 .. l0 + 3][q2 lanes], padded
+  using namespace n2k;
+  const int s = blockIdx.x, l0 = blockIdx.y * 4, b = blockIdx.z;
+  // position x of factor p holds natural slot brv(x)
+  for (int x = threadIdx.x; x < 2 * N; x += EPI_NT) {
+    const int p = x >> 11, xx = x & (N - 1);
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(
+        fin + ((((size_t)b * nshards + s) * 2 + p) * N + __ldg(uof + brv11(xx))) * SIMD + l0));
+    uint32_t* o = sm + 4 * p * PS + phys(xx);
+    o[0] = v.x, o[PS] = v.y, o[2 * PS] = v.z, o[3 * PS] = v.w;
+  }
+  __syncthreads();
+  inv<EPI_NT>(sm, 4, 4, T);
+  const int ds = distinct_of[s];
+  // the secondary input of queries [c * chunk, ...) is one [t][lanes_c][N] block
+  const int c = b / chunk, bl = b % chunk;
+  const size_t lanes_c = (size_t)CTXT_PARTS * min(chunk, nq - c * chunk);
+  uint16_t* const base = sec_in + (size_t)c * chunk * CTXT_PARTS * nshards * SIMD * N;
+  for (int x = threadIdx.x; x < 4 * N; x += EPI_NT) {
+    const int ll = x >> 11, n = x & (N - 1);
+    const uint32_t o = phys(n);
+    const uint32_t x1 = shoup_mul(sm[ll * PS + o], k1, k1q, P1);
+    const uint32_t x2 = shoup_mul(sm[(4 + ll) * PS + o], k2, k2q, P2);
+    uint64_t v = (uint64_t)x1 * P2 + (uint64_t)x2 * P1;
+    v = v >= QQ ? v - QQ : v;
+    const uint32_t aq = __ldg(a_ms + ((size_t)ds * SIMD + l0 + ll) * N + n);
+    uint32_t w = (aq << PRIM_B_BITS) + ms_encode12(v);
+    const uint32_t d0 = w % TPLAIN;
+    w /= TPLAIN;
+    const uint32_t d1 = w % TPLAIN;
+    const uint32_t d2 = w / TPLAIN;
+    uint16_t* op = base + (((size_t)s * SIMD + l0 + ll) * lanes_c + (size_t)bl * CTXT_PARTS) * N + n;
+    op[0] = (uint16_t)d0;
+    op[N] = (uint16_t)d1;
+    op[2 * N] = (uint16_t)d2;
+  }
+}
+
 __global__ void epilogue_zq_kernel(const uint32_t* __restrict__ part, int chunks, uint64_t* __restrict__ out,
                                    Group g, const uint32_t* __restrict__ uof, NttTables T, CrtConst crtc) {
   extern __shared__ uint32_t sm[];
@@ -308,6 +371,16 @@ void launch_scan_lanes(const uint32_t* slab, const uint32_t* qlane, uint32_t* pa
 void launch_primary_epilogue(const uint32_t* fin, int nq, int nshards, const uint32_t* a_ms, const int* distinct_of,
                              uint16_t* sec_in, int chunk, const Group& g, const SlotMaps& maps, const NttTables& T,
                              cudaStream_t st) {
+  if (g.log2n == 11) {
+    const CrtConst cc = host_crt_const();
+    const uint32_t k1q = (uint32_t)(((uint64_t)cc.q2inv1 << 32) / P1);
+    const uint32_t k2q = (uint32_t)(((uint64_t)cc.q1inv2 << 32) / P2);
+    const size_t smem = (size_t)8 * n2k::PS * 4;
+    set_smem(primary_epilogue2k_kernel, smem);
+    primary_epilogue2k_kernel<<<dim3(nshards, SIMD / 4, nq), EPI_NT, smem, st>>>(
+        fin, nshards, a_ms, distinct_of, sec_in, nq, chunk, maps.uof, T, cc.q2inv1, k1q, cc.q1inv2, k2q);
+    return;
+  }
   const size_t smem = (size_t)4 * g.n * 4;
   dim3 grid(nshards, SIMD / 2, nq);
   set_smem(primary_epilogue_kernel, smem);
