@@ -144,6 +144,21 @@ int presize(Db& db) {
   return DNSPIR_OK;
 }
 
+// Group sizes come from a fixed set -- 1, 2, 3, 4, 6, 8, 12, ... (powers of
+// two and 1.5 times powers of two) and the admitted maximum -- so that at most
+// about 2 log2(max) sizes ever run, each captured once per slot: the first
+// group of a size runs directly and holds the worker while its graphs are
+// captured and instantiated.  The smallest member not below n (n <= cap); a
+// group is padded up to it rather than leaving queries for the next group,
+// since a group's pass over the slabs costs the same whatever its size.
+int group_size_ceil(int n, int cap) {
+  for (int p = 1; p < cap; p *= 2) {
+    if (p >= n) return p;
+    if (p >= 2 && p + p / 2 >= n && p + p / 2 < cap) return p + p / 2;
+  }
+  return cap;
+}
+
 // Launch one group of db on slot k: staging, H2D, primary and secondary
 // phases (graphs when captured), completion event.
 int launch_group(dnspir_server* sv, Db& db, int k, const std::vector<Request*>& rq) {
@@ -287,6 +302,12 @@ void worker_main(dnspir_server* sv) {
         }
       }
       if (rq.empty()) continue;
+      // fill the group up to the next size of the set with copies of its last
+      // query; their replies go to ticket 0, which no request has
+      for (int target = group_size_ceil((int)rq.size(), db.admitted); (int)rq.size() < target;) {
+        rq.push_back(rq.back());
+        tk.push_back(0);
+      }
       idle = false;
       db.inflight[k].busy = true;
       db.inflight[k].tickets = tk;
