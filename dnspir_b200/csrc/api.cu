@@ -142,7 +142,9 @@ static DeviceCtx* g_ctx[64];
 
 static int build_tables(DeviceCtx& c) {
   const int n = N_MAX;
-  std::vector<uint32_t> h(8 * n);
+  // 8 scalar tables (fw, fwq, iw, iwq of each factor), then the pairs
+  // (w, Shoup companion) interleaved: fw2 of each factor, iw2 of each factor
+  std::vector<uint32_t> h(16 * n);
   for (int pi = 0; pi < 2; pi++) {
     const uint64_t p = pi ? P2 : P1;
     const uint64_t zeta = prim_root_2n(p, 2 * n);
@@ -154,6 +156,10 @@ static int build_tables(DeviceCtx& c) {
       h[(2 + pi) * n + k] = (uint32_t)(((u128)f << 32) / p);
       h[(4 + pi) * n + k] = (uint32_t)iv;
       h[(6 + pi) * n + k] = (uint32_t)(((u128)iv << 32) / p);
+      h[(8 + 2 * pi) * n + 2 * k] = h[(0 + pi) * n + k];
+      h[(8 + 2 * pi) * n + 2 * k + 1] = h[(2 + pi) * n + k];
+      h[(12 + 2 * pi) * n + 2 * k] = h[(4 + pi) * n + k];
+      h[(12 + 2 * pi) * n + 2 * k + 1] = h[(6 + pi) * n + k];
     }
     for (int lg = 0; lg <= LOG2_N_MAX; lg++) {
       const uint64_t ni = invmod((1ull << lg) % p, p);
@@ -168,6 +174,8 @@ static int build_tables(DeviceCtx& c) {
     c.T.fwq[pi] = c.tables + (2 + pi) * n;
     c.T.iw[pi] = c.tables + (4 + pi) * n;
     c.T.iwq[pi] = c.tables + (6 + pi) * n;
+    c.T.fw2[pi] = reinterpret_cast<const uint2*>(c.tables + (8 + 2 * pi) * n);
+    c.T.iw2[pi] = reinterpret_cast<const uint2*>(c.tables + (12 + 2 * pi) * n);
   }
   return DNSPIR_OK;
 }

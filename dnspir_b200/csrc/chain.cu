@@ -750,6 +750,10 @@ __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
       kc[f][3][m] = mont_reduce((uint64_t)qq[o] * cp.r2, cp.p, cp.pinv);
       kc[f][4][m] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
       kc[f][5][m] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+      // with t = sigma_5(a): NTT(d0) gk0 + NTT(d1) gk1 = t gk0 + NTT(d1) (gk1 - 2^26 gk0),
+      // and likewise for the b-part keys, so the pointwise stage needs no d0
+      kc[f][1][m] = sub_mod(kc[f][1][m], mont_reduce((uint64_t)kc[f][0][m] * cp.c26, cp.p, cp.pinv), cp.p);
+      kc[f][4][m] = sub_mod(kc[f][4][m], mont_reduce((uint64_t)kc[f][3][m] * cp.c26, cp.p, cp.pinv), cp.p);
     }
   }
   __syncthreads();  // the table in D is overwritten by the first step
@@ -770,14 +774,12 @@ __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
     // inverse stages 0-1 from registers
 #pragma unroll
     for (int f = 0; f < 2; f++) {
-      const uint32_t* __restrict__ iw = a.T.iw[f];
-      const uint32_t* __restrict__ iwq = a.T.iwq[f];
+      const Tw4 w = load_tw4(a.T.iw2[f], tid);
       uint4 v = make_uint4(ta[f][0], ta[f][1], ta[f][2], ta[f][3]);
-      gs(v.x, v.y, __ldg(iw + 1024 + 2 * tid), __ldg(iwq + 1024 + 2 * tid), pr[f]);
-      gs(v.z, v.w, __ldg(iw + 1024 + 2 * tid + 1), __ldg(iwq + 1024 + 2 * tid + 1), pr[f]);
-      const uint32_t w = __ldg(iw + 512 + tid), wq = __ldg(iwq + 512 + tid);
-      gs(v.x, v.z, w, wq, pr[f]);
-      gs(v.y, v.w, w, wq, pr[f]);
+      gs(v.x, v.y, w.b0, w.b0q, pr[f]);
+      gs(v.z, v.w, w.b1, w.b1q, pr[f]);
+      gs(v.x, v.z, w.a, w.aq, pr[f]);
+      gs(v.y, v.w, w.a, w.aq, pr[f]);
       *reinterpret_cast<uint4*>(D + f * PS + qb) = v;
     }
     __syncthreads();
@@ -793,7 +795,7 @@ __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
       uint32_t* y = D + f * PS + base;
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = y[k * STR];
-      inv8_bf(v, load_tw8(a.T.iw[f], a.T.iwq[f], 1, 0), pr[f]);
+      inv8_bf(v, load_tw8(a.T.iw2[f], 1, 0), pr[f]);
 #pragma unroll
       for (int k = 0; k < 8; k++) y[k * STR] = v[k];
       __syncthreads();
@@ -804,7 +806,7 @@ __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
         const int32_t hd = f == 0 ? high_digit(v[k], o, a.cp[0], a.cp[1]) : high_digit(o, v[k], a.cp[0], a.cp[1]);
         v[k] = hd < 0 ? (uint32_t)(hd + (int32_t)pr[f]) : (uint32_t)hd;
       }
-      fwd8_bf(v, load_tw8(a.T.fw[f], a.T.fwq[f], 1, 0), pr[f]);
+      fwd8_bf(v, load_tw8(a.T.fw2[f], 1, 0), pr[f]);
       uint32_t* w = A + f * PS + base;
 #pragma unroll
       for (int k = 0; k < 8; k++) w[k * STR] = v[k];
@@ -817,25 +819,22 @@ __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
     for (int f = 0; f < 2; f++) {
       const ChainPrime& cp = a.cp[f];
       const uint32_t p = pr[f];
-      const uint32_t* __restrict__ fw = a.T.fw[f];
-      const uint32_t* __restrict__ fwq = a.T.fwq[f];
+      const Tw4 w = load_tw4(a.T.fw2[f], tid);
       uint4 v = *reinterpret_cast<const uint4*>(A + f * PS + qb);
-      const uint32_t w = __ldg(fw + 512 + tid), wq = __ldg(fwq + 512 + tid);
-      ct(v.x, v.z, w, wq, p);
-      ct(v.y, v.w, w, wq, p);
-      ct(v.x, v.y, __ldg(fw + 1024 + 2 * tid), __ldg(fwq + 1024 + 2 * tid), p);
-      ct(v.z, v.w, __ldg(fw + 1024 + 2 * tid + 1), __ldg(fwq + 1024 + 2 * tid + 1), p);
+      ct(v.x, v.z, w.a, w.aq, p);
+      ct(v.y, v.w, w.a, w.aq, p);
+      ct(v.x, v.y, w.b0, w.b0q, p);
+      ct(v.z, v.w, w.b1, w.b1q, p);
       const uint32_t n1s[4] = {red(red(v.x, 2 * p), p), red(red(v.y, 2 * p), p), red(red(v.z, 2 * p), p),
                                red(red(v.w, 2 * p), p)};
       const uint32_t es[4] = {e[f].x, e[f].y, e[f].z, e[f].w};
       uint32_t an[4], bn[4];
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        const uint32_t n1 = n1s[m];
-        const uint32_t n0 = sub_mod(ta[f][m], mont_reduce((uint64_t)n1 * cp.c26, p, cp.pinv), p);
-        an[m] = mont_reduce((uint64_t)n0 * kc[f][0][m] + (uint64_t)n1 * kc[f][1][m] + (uint64_t)es[m] * kc[f][2][m], p,
+        const uint32_t n1 = n1s[m], t = ta[f][m];
+        an[m] = mont_reduce((uint64_t)t * kc[f][0][m] + (uint64_t)n1 * kc[f][1][m] + (uint64_t)es[m] * kc[f][2][m], p,
                             cp.pinv);
-        bn[m] = mont_reduce(((uint64_t)tb[f][m] << 32) + (uint64_t)n0 * kc[f][3][m] + (uint64_t)n1 * kc[f][4][m] +
+        bn[m] = mont_reduce(((uint64_t)tb[f][m] << 32) + (uint64_t)t * kc[f][3][m] + (uint64_t)n1 * kc[f][4][m] +
                                 (uint64_t)es[m] * kc[f][5][m],
                             p, cp.pinv);
       }

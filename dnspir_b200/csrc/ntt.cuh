@@ -22,6 +22,8 @@ struct NttTables {
   const uint32_t* fwq[2];  // shoup companions
   const uint32_t* iw[2];   // psi^-brv(k)
   const uint32_t* iwq[2];
+  const uint2* fw2[2];     // (psi^brv(k), companion) pairs, for vector loads
+  const uint2* iw2[2];
   uint32_t ninv[2][LOG2_N_MAX + 1];   // n^-1 mod p for n = 2^i
   uint32_t ninvq[2][LOG2_N_MAX + 1];
 };

@@ -55,15 +55,30 @@ struct Geo8 {
 struct Tw8 {
   uint32_t a, aq, b[2], bq[2], c[4], cq[4];
 };
-__device__ __forceinline__ Tw8 load_tw8(const uint32_t* __restrict__ tw, const uint32_t* __restrict__ twq, int M,
-                                        int blk) {
+// The seven twiddles of a radix-8 group from the interleaved (w, companion)
+// table: one 8-byte and three 16-byte loads (2M + 2 blk and 4M + 4 blk are
+// even, so the pairs of pairs are 16-byte aligned).
+__device__ __forceinline__ Tw8 load_tw8(const uint2* __restrict__ tw2, int M, int blk) {
   Tw8 t;
-  t.a = __ldg(tw + M + blk), t.aq = __ldg(twq + M + blk);
-#pragma unroll
-  for (int j = 0; j < 2; j++) t.b[j] = __ldg(tw + 2 * M + 2 * blk + j), t.bq[j] = __ldg(twq + 2 * M + 2 * blk + j);
-#pragma unroll
-  for (int j = 0; j < 4; j++) t.c[j] = __ldg(tw + 4 * M + 4 * blk + j), t.cq[j] = __ldg(twq + 4 * M + 4 * blk + j);
+  const uint2 a = __ldg(tw2 + M + blk);
+  const uint4 b = __ldg(reinterpret_cast<const uint4*>(tw2 + 2 * M + 2 * blk));
+  const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(tw2 + 4 * M + 4 * blk));
+  const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(tw2 + 4 * M + 4 * blk + 2));
+  t.a = a.x, t.aq = a.y;
+  t.b[0] = b.x, t.bq[0] = b.y, t.b[1] = b.z, t.bq[1] = b.w;
+  t.c[0] = c0.x, t.cq[0] = c0.y, t.c[1] = c0.z, t.cq[1] = c0.w;
+  t.c[2] = c1.x, t.cq[2] = c1.y, t.c[3] = c1.z, t.cq[3] = c1.w;
   return t;
+}
+// The three twiddles of the radix-4 pass on quad g: tw[512 + g] and the pair
+// tw[1024 + 2g], tw[1024 + 2g + 1].
+struct Tw4 {
+  uint32_t a, aq, b0, b0q, b1, b1q;
+};
+__device__ __forceinline__ Tw4 load_tw4(const uint2* __restrict__ tw2, int g) {
+  const uint2 a = __ldg(tw2 + 512 + g);
+  const uint4 b = __ldg(reinterpret_cast<const uint4*>(tw2 + 1024 + 2 * g));
+  return Tw4{a.x, a.y, b.x, b.y, b.z, b.w};
 }
 
 __device__ __forceinline__ void fwd8_bf(uint32_t (&v)[8], const Tw8& t, uint32_t p) {
@@ -122,7 +137,7 @@ __device__ __forceinline__ void pass8(uint32_t* x, int cnt0, int cnt1, const Ntt
       const int lo = pi ? cnt0 : 0, hi = pi ? cnt0 + cnt1 : cnt0;
       if (lo >= hi) continue;
       const uint32_t p = prime_of(pi);
-      const Tw8 t = INV ? load_tw8(T.iw[pi], T.iwq[pi], M, blk) : load_tw8(T.fw[pi], T.fwq[pi], M, blk);
+      const Tw8 t = load_tw8(INV ? T.iw2[pi] : T.fw2[pi], M, blk);
       for (int poly = lo + po; poly < hi; poly += S::PPI) {
         uint32_t* y = x + poly * PS + base;
         uint32_t v[8];
@@ -161,11 +176,8 @@ __device__ __forceinline__ void pass4(uint32_t* x, int cnt0, int cnt1, const Ntt
       const int lo = pi ? cnt0 : 0, hi = pi ? cnt0 + cnt1 : cnt0;
       if (lo >= hi) continue;
       const uint32_t p = prime_of(pi);
-      const uint32_t* __restrict__ tw = INV ? T.iw[pi] : T.fw[pi];
-      const uint32_t* __restrict__ twq = INV ? T.iwq[pi] : T.fwq[pi];
-      const uint32_t a = __ldg(tw + 512 + g), aq = __ldg(twq + 512 + g);
-      const uint32_t b0 = __ldg(tw + 1024 + 2 * g), b0q = __ldg(twq + 1024 + 2 * g);
-      const uint32_t b1 = __ldg(tw + 1024 + 2 * g + 1), b1q = __ldg(twq + 1024 + 2 * g + 1);
+      const Tw4 tw = load_tw4(INV ? T.iw2[pi] : T.fw2[pi], g);
+      const uint32_t a = tw.a, aq = tw.aq, b0 = tw.b0, b0q = tw.b0q, b1 = tw.b1, b1q = tw.b1q;
       for (int poly = lo + po; poly < hi; poly += S::PPI) {
         uint4* y = reinterpret_cast<uint4*>(x + poly * PS + base);
         uint4 v = *y;
