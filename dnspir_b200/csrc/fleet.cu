@@ -220,6 +220,9 @@ int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_de
   for (int c0 = 0; c0 < nb; c0 += f->sec_chunk) {
     const int nc = std::min(f->sec_chunk, nb - c0);
     const int nl = CTXT_PARTS * nc;
+    // the last chunk's start: a later group's primary phase may wait for this
+    // instead of the whole phase (it then shares the SMs the last chunk leaves idle)
+    if (c0 + f->sec_chunk >= nb && s.sec_tail) CK(cudaEventRecord(s.sec_tail, st));
     const uint16_t* in = s.sec_in.as<uint16_t>() + (size_t)c0 * CTXT_PARTS * l_in * n;
     launch_encode_cols(in, f->secE.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
     launch_encode_rows(f->secE.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
@@ -306,6 +309,7 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   for (auto& s : f->slot) {
     CK(cudaEventCreateWithFlags(&s.prim_done, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&s.sec_done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s.sec_tail, cudaEventDisableTiming));
   }
   f->slabs.assign(num_distinct, nullptr);
   f->ready.assign(num_distinct, false);
@@ -499,18 +503,19 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
     }
   }
   // schedule: the best shape again with each group's primary phase waiting for
-  // the previous group's secondary phase; keep whichever is faster
-  bool serial = false;
-  if (rc == DNSPIR_OK && best_i >= 0) {
+  // the previous group's secondary phase (1), or for its last chunk (2); keep
+  // whichever of the three is fastest
+  int serial = 0;
+  for (int sched = 1; sched <= 2 && rc == DNSPIR_OK && best_i >= 0; sched++) {
     f->tuned[nb] = best_i;
-    f->tuned_serial[nb] = 1;
+    f->tuned_serial[nb] = sched;
     rc = dnspir_fleet_process_queries(f, ptrs.data(), lens.data(), (uint32_t)(nb * groups), r.as<uint8_t>(), RB,
                                       nullptr, 1);
     if (rc == DNSPIR_OK) {
       std::lock_guard<std::mutex> lk(f->mu);
       float t = 0;
       if (cudaEventElapsedTime(&t, f->tev[6], f->tev[17]) == cudaSuccess && t / 2 < best) {
-        serial = true;
+        serial = sched;
         best = t / 2;
         if (ms_per_shape) ms_per_shape[best_i] = best;
       }
@@ -523,7 +528,7 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
   if (rc != DNSPIR_OK) return rc;
   if (best_i < 0) return fail(DNSPIR_ERR_CUDA, "no tile shape ran");
   f->tuned[nb] = best_i;
-  f->tuned_serial[nb] = serial ? 1 : 0;
+  f->tuned_serial[nb] = serial;
   if (chosen) *chosen = best_i;
   return DNSPIR_OK;
 }
@@ -720,10 +725,12 @@ int dnspir_fleet_process_queries(dnspir_fleet* f, const uint8_t* const* queries,
     CKR(group_events(f, gi, &t));
     CKR(slot_acquire(f, s));
     // schedule: unless this group size overlaps, its primary phase waits for
-    // the previous group's secondary phase (the two phases then do not share SMs)
+    // the previous group's secondary phase (the two phases then do not share
+    // SMs), or for that phase to reach its last chunk
     auto so = f->tuned_serial.find(nb);
-    if (so != f->tuned_serial.end() && so->second && f->slot[(gi & 1) ^ 1].sec_pending)
-      CK(cudaStreamWaitEvent(f->st, f->slot[(gi & 1) ^ 1].sec_done, 0));
+    const QSlot& prev = f->slot[(gi & 1) ^ 1];
+    if (so != f->tuned_serial.end() && so->second && prev.sec_pending)
+      CK(cudaStreamWaitEvent(f->st, so->second == 2 ? prev.sec_tail : prev.sec_done, 0));
     CKR(fleet_slot_workspace(f, s, Bk, nb, (size_t)nb * want));
     // host staging of the slot may still feed the copies of the group two back
     if (s.prim_recorded) CK(cudaEventSynchronize(s.prim_done));
@@ -803,6 +810,7 @@ int dnspir_fleet_perform_double_pir(dnspir_fleet* f, const uint64_t* pq, const u
   QSlot s;
   CK(cudaEventCreateWithFlags(&s.prim_done, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&s.sec_done, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s.sec_tail, cudaEventDisableTiming));
   for (auto& o : f->slot) CKR(slot_acquire(f, o));
   const int Bk = fleet_kernel_batch(f, 1);
   cudaEvent_t* t = nullptr;

@@ -14,6 +14,7 @@ struct QSlot {
   DBuf qbytes, qdesc, qnat, qbrv, fin, sec_in, reply_dev;
   HBuf qpin, dpin, rpin;  // host staging: query bytes, descriptors, reply bytes
   cudaEvent_t prim_done = nullptr, sec_done = nullptr;
+  cudaEvent_t sec_tail = nullptr;  // the secondary phase has reached its last chunk
   bool sec_pending = false, prim_recorded = false;
   // captured launch sequences of the serving loop, per group size
   std::map<int, cudaGraphExec_t> gprim, gsec;
@@ -27,6 +28,7 @@ struct QSlot {
     drop_graphs();
     if (prim_done) cudaEventDestroy(prim_done);
     if (sec_done) cudaEventDestroy(sec_done);
+    if (sec_tail) cudaEventDestroy(sec_tail);
   }
 };
 
@@ -54,7 +56,9 @@ struct dnspir_fleet {
   dnspir::DBuf qb, err_word, tmp_lane;        // tensor engine: query operand, wait-error word, preprocessing scratch
   std::map<int, int> tuned;                   // tensor engine: group size -> tile shape index
   std::map<int, int> tuned_cc;                // CUDA-core engine: group size -> queries per block
-  std::map<int, int> tuned_serial;            // group size -> 1: primary waits for the previous secondary
+  std::map<int, int> tuned_serial;            // group size -> schedule: 0 the primary phase overlaps the previous
+                                              // group's secondary, 1 waits for all of it, 2 waits until it
+                                              // reaches its last chunk
   std::vector<cudaEvent_t> tev;               // 6 timing events per group of the last call
   std::vector<int> q_group;                   // per query of the last call: its group, or -1
   std::mutex mu;
