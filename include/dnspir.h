@@ -144,7 +144,8 @@ int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, ui
  * phase of one group overlaps the scan of the next.  ms_per_shape receives
  * milliseconds per group.  The schedule is tuned too: the best shape is timed
  * again with each group's primary phase waiting for the previous group's
- * secondary phase, and that schedule is kept for the group size when faster. */
+ * secondary phase, and again waiting only until that phase starts its last
+ * chunk; the fastest of the three schedules is kept for the group size. */
 int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
 /* CUDA-core engine: time the scan of a group of `batch` queries (a power of two
  * up to 256, one launch) with 1, 2, 4, 8 and 16 queries per block and keep the
