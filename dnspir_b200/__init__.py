@@ -90,6 +90,7 @@ def lib():
         L.dnspir_tscan_shapes.argtypes = [_vp, _vp, _vp, _vp, c.c_int]
         L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
         L.dnspir_fleet_set_tile.argtypes = [_vp, c.c_uint32, c.c_int]
+        L.dnspir_fleet_set_schedule.argtypes = [_vp, c.c_uint32, c.c_int]
         L.dnspir_fleet_tune_pipeline.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_fleet_tune_cuda_cores.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
@@ -389,6 +390,12 @@ class Fleet:
     def set_tile(self, batch, shape_index):
         """Tensor engine: tile shape index for groups of `batch` (-1: default)."""
         _check(lib().dnspir_fleet_set_tile(self._h, batch, shape_index))
+
+    def set_schedule(self, batch, schedule):
+        """How groups of `batch` follow the previous group: 0 overlap its
+        secondary phase, 1 wait for all of it, 2 wait for its last chunk to
+        start, -1 the default."""
+        _check(lib().dnspir_fleet_set_schedule(self._h, batch, schedule))
 
     def set_engine(self, engine):
         """ENGINE_CUDA_CORES or ENGINE_TENSOR; marks every shard unprepared."""

@@ -588,6 +588,19 @@ int dnspir_fleet_tune_cuda_cores(dnspir_fleet* f, uint32_t batch, double* ms_per
   return DNSPIR_OK;
 }
 
+int dnspir_fleet_set_schedule(dnspir_fleet* f, uint32_t batch, int schedule) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
+  if (batch < 1 || batch > (uint32_t)TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
+  if (schedule < -1 || schedule > 2) return fail(DNSPIR_ERR_BAD_ARG, "schedule must be -1, 0, 1 or 2");
+  if (schedule < 0)
+    f->tuned_serial.erase((int)batch);
+  else
+    f->tuned_serial[(int)batch] = schedule;
+  return DNSPIR_OK;
+}
+
 int dnspir_fleet_set_tile(dnspir_fleet* f, uint32_t batch, int shape_index) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
   std::lock_guard<std::mutex> lk(f->mu);

@@ -152,6 +152,12 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_p
  * fastest; ms_per_tile[5] receives the times (-1 when not run), *chosen the
  * queries per block.  No counterpart in the reference. */
 int dnspir_fleet_tune_cuda_cores(dnspir_fleet* fleet, uint32_t batch, double* ms_per_tile, int* chosen);
+/* How a group of `batch` queries follows the previous group, overriding the
+ * default or a previous tune: 0 its primary phase overlaps the previous
+ * group's secondary phase, 1 it waits for all of that phase, 2 it waits until
+ * that phase starts its last chunk; -1 returns to the default (0).  Either
+ * engine.  No counterpart in the reference. */
+int dnspir_fleet_set_schedule(dnspir_fleet* fleet, uint32_t batch, int schedule);
 /* Tensor engine: use tile shape `shape_index` (dnspir_tscan_shapes order) for
  * groups of `batch` queries, overriding the table or a previous tune; -1
  * returns to the default.  No counterpart in the reference. */

@@ -273,6 +273,30 @@ def test_full_secondary_group_matches_oracle(full_secondary, batch, nq):
         assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), (i, j)
 
 
+@pytest.mark.parametrize("schedule", [0, 1, 2])
+def test_group_schedules_keep_replies(full_secondary, schedule):
+    # 64 queries answered as two groups of 32 in one call; each group's
+    # secondary phase runs in two chunks (24 + 8 queries), and the second
+    # group's primary phase overlaps the first group's secondary phase (0),
+    # waits for all of it (1) or for its last chunk to start (2).  Every reply
+    # decrypts; one per group is compared with the oracle byte for byte.
+    data, refs, fleet, l1, l2, count = full_secondary
+    rng = orc.Rng(bytes([9, schedule]) + bytes(30))
+    picks = [((53 * k + 11 * schedule) % (8 * l1), (71 * k + schedule) % count) for k in range(64)]
+    qs = [orc.prepare_query(rng, i, j, l1, l2) for i, j in picks]
+    fleet.set_batch(32)
+    fleet.set_schedule(32, schedule)
+    try:
+        got = fleet.process_queries([q for q, _ in qs])
+    finally:
+        fleet.set_schedule(32, -1)
+        fleet.set_batch(1)
+    for k, ((i, j), (q, seed), r) in enumerate(zip(picks, qs, got)):
+        if k in (31, 63):
+            assert r == orc.process_query(refs, q), k
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), k
+
+
 def test_full_secondary_group_large_chunk(full_secondary):
     # 16 queries: their secondary chains no longer fit one block per SM as
     # 2-block clusters, so the one-block-per-part kernel runs; three replies
