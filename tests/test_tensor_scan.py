@@ -163,3 +163,33 @@ def test_every_tile_shape_equals_cuda_core_scan(config1_pair):
     finally:
         fb.set_tile(10, -1)
         fb.set_batch(1)
+
+
+def test_engines_agree_at_full_size():
+    # the shape of 2^22 entries: 256 full shards of order 2048 (on 2 distinct
+    # shards in HBM) and the full secondary group.  The oracle would take
+    # minutes per query here, so two size-independent properties stand in:
+    # the tensor engine's replies equal the CUDA-core engine's byte for byte
+    # (one query at a time there, groups of 4 on the tensor cores), and every
+    # reply decrypts to its entry.
+    entries = 1 << 22
+    l1, l2, shards = dp.get_database_shape(entries)
+    assert (l1, l2, shards) == (2048, 2048, 256)
+    data = np.stack([_data(900 + i, 8 * l1, 2048) for i in range(2)])
+    fa = dp.Fleet(entries, 2)
+    fa.set_shards(0, data)
+    fb = dp.Fleet(entries, 2)
+    fb.set_engine(dp.ENGINE_TENSOR)
+    fb.set_shards(0, data)
+    rng = orc.Rng(bytes([11]) + bytes(31))
+    picks = [(0, 0), (8 * l1 - 1, 255), (4097, 128), (12345, 3), (777, 201)]
+    qs = [orc.prepare_query(rng, i, j, l1, l2) for i, j in picks]
+    ra = fa.process_queries([q for q, _ in qs])
+    fb.set_batch(4)
+    try:
+        rb = fb.process_queries([q for q, _ in qs])
+    finally:
+        fb.set_batch(1)
+    for (i, j), (q, seed), a, b in zip(picks, qs, ra, rb):
+        assert a == b, (i, j)
+        assert np.array_equal(orc.process_reply(a, seed), data[j % 2][i].astype(np.int64)), (i, j)
