@@ -193,3 +193,23 @@ def test_engines_agree_at_full_size():
     for (i, j), (q, seed), a, b in zip(picks, qs, ra, rb):
         assert a == b, (i, j)
         assert np.array_equal(orc.process_reply(a, seed), data[j % 2][i].astype(np.int64)), (i, j)
+
+
+def test_empty_call_and_largest_group(config1_pair):
+    # no queries: nothing to answer, no error; then the largest group the
+    # tensor engine takes (256 queries in one pass over the slabs): every
+    # reply decrypts, and a sample equals the oracle's bytes
+    data, fa, fb, refs, l1, l2, shards = config1_pair
+    assert fb.process_queries([]) == []
+    rng = orc.Rng(bytes([12]) + bytes(31))
+    picks = [((2897 * k + 1) % (8 * l1), k % shards) for k in range(256)]
+    qs = [orc.prepare_query(rng, i, j, l1, l2) for i, j in picks]
+    fb.set_batch(256)
+    try:
+        got = fb.process_queries([q for q, _ in qs])
+    finally:
+        fb.set_batch(1)
+    for k, ((i, j), (q, seed), r) in enumerate(zip(picks, qs, got)):
+        if k % 37 == 0 or k == 255:
+            assert r == orc.process_query(refs, q), k
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), k
