@@ -2,6 +2,8 @@
 
 Restates, against oracle/dnspir_oracle.cpp:
   * the N = 8 layout known-answer tests (crates/pir/src/base_pir.rs:1281-1411),
+    from tests/golden/kat_layout_n8.json (extracted from the reference's test
+    source by tests/golden/make_golden.py),
   * the decrypt-equality tests at N = 256 (base_pir.rs:1413-1537,
     double_pir.rs:328-451),
   * the codec round trip (pir_wrapper.rs:442-452),
@@ -9,6 +11,9 @@ Restates, against oracle/dnspir_oracle.cpp:
   * the shape rules (pir_wrapper.rs:166-241) against the reference's own run
     log (ARTIFACT-APPENDIX.md:141-142) and wire sizes (:163-165).
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -44,31 +49,23 @@ def _unit(n, count, idx, poly):
 
 ONE8 = [1, 0, 0, 0, 0, 0, 0, 0]
 X8 = [0, 1, 0, 0, 0, 0, 0, 0]
-M1 = T - 1
 
 
-@pytest.mark.parametrize("l,count,factor", [(8, 64, 8), (4, 32, 4)])
-def test_set_transformed_entries_full_and_g_subgroup(l, count, factor):
-    # base_pir.rs:1281-1367 (full group and the order-4 subgroup share expectations)
-    db = orc.Database(3, l)
-    db.set_transformed_entries(_unit(8, count, 0, ONE8))
-    _check_layout(db, [ONE8] * 4, factor)
-    db.set_transformed_entries(_unit(8, count, 8, ONE8))
-    _check_layout(db, [[0, 0, 0, 0, 0, 0, 0, M1]] * 4, factor)
-    db.set_transformed_entries(_unit(8, count, 0, X8))
-    _check_layout(db, [[0, 0, 0, 0, 0, 1, 0, 0], [0, M1, 0, 0, 0, 0, 0, 0],
-                       [0, 0, 0, 0, 0, M1, 0, 0], [0, 1, 0, 0, 0, 0, 0, 0]], factor)
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "kat_layout_n8.json")
+KAT = json.load(open(GOLDEN))
 
 
-def test_set_transformed_entries_small_subgroup():
-    # base_pir.rs:1369-1411
-    db = orc.Database(3, 2)
-    db.set_transformed_entries(_unit(8, 16, 0, ONE8))
-    _check_layout(db, [ONE8] * 2, 2)
-    db.set_transformed_entries(_unit(8, 16, 8, ONE8))
-    _check_layout(db, [[0, 0, 0, 0, 0, 0, M1, 0]] * 2, 2)
-    db.set_transformed_entries(_unit(8, 16, 0, X8))
-    _check_layout(db, [[0, 0, 0, 0, 0, M1, 0, 0], [0, 1, 0, 0, 0, 0, 0, 0]], 2)
+@pytest.mark.parametrize("name", sorted(KAT["tests"]))
+def test_set_transformed_entries_known_answers(name):
+    # base_pir.rs:1281-1411, the cases read from the reference's test source
+    # by tests/golden/make_golden.py: full group, order-4 and order-2 subgroups
+    kat = KAT["tests"][name]
+    db = orc.Database(kat["log2n"], kat["order"])
+    for case in kat["cases"]:
+        poly = ONE8 if case["entry"] == "1" else X8
+        db.set_transformed_entries(_unit(8, case["count"], case["index"], poly))
+        rows = [[x % T for x in row] for row in case["rows"]]
+        _check_layout(db, rows, kat["factor"])
 
 
 def _monomial(n, e):
