@@ -51,10 +51,11 @@ __device__ __forceinline__ void ld_lanes(const uint32_t* p, uint32_t* v, int lpt
 }
 
 // 16 queries per block: two blocks per SM (128 registers, 16 warps: the
-// kernel is latency-bound at one block of 8 warps); the smaller shapes would
-// spill under that bound and keep one
+// kernel is latency-bound at one block of 8 warps); the other shapes would
+// spill under that bound and keep the compiler's own register choice (a
+// minimum of 0 blocks leaves it as with no minimum)
 template <int B, int LPT>
-__global__ void __launch_bounds__(SCAN_NT, B == 16 ? 2 : 1) scan_batch_kernel(ScanArgs a) {
+__global__ void __launch_bounds__(SCAN_NT, B == 16 ? 2 : 0) scan_batch_kernel(ScanArgs a) {
   constexpr int LG = SIMD / LPT;     // lane groups per slot
   constexpr int TS = SCAN_NT / LG;   // slots per tile
   extern __shared__ uint32_t win[];  // [3][B][W]: x fastest, so a warp's slots hit distinct banks
