@@ -394,7 +394,8 @@ class Fleet:
     def set_schedule(self, batch, schedule):
         """How groups of `batch` follow the previous group: 0 overlap its
         secondary phase, 1 wait for all of it, 2 wait for its last chunk to
-        start, -1 the default."""
+        start; plus 4 for two-block-cluster chains at every chunk size; -1 the
+        default."""
         _check(lib().dnspir_fleet_set_schedule(self._h, batch, schedule))
 
     def set_engine(self, engine):

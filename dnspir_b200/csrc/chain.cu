@@ -978,7 +978,8 @@ void launch_primary_finalize(const uint32_t* a_out, int nshards, uint64_t* a_zq,
 }
 
 void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_stride, int nq, uint32_t* out,
-                            const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st) {
+                            const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st,
+                            bool clustered) {
   ChainArgs a = chain_args(g, cc, T);
   a.E = E;
   a.qv = qv;
@@ -989,12 +990,14 @@ void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_str
   // for a few queries: the chains run on many SMs, and a block fits beside a
   // scan block) while the chunk needs at most one block per SM; beyond that one
   // block per part carrying both factors (no cluster barrier, twice the work
-  // per barrier): at N = 2048 the register-transform kernel, else the generic one
+  // per barrier): at N = 2048 the register-transform kernel, else the generic one.
+  // `clustered` asks for the cluster form at any chunk size (it shares SMs with
+  // a running scan; the pipeline tuner picks it per group size when faster)
   int sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool full = g.log2n == LOG2_N_MAX;
-  if ((long)nq * CTXT_PARTS * g.H * 2 <= sms) {
+  if (clustered || (long)nq * CTXT_PARTS * g.H * 2 <= sms) {
     const size_t smem = chain_smem(g, 1);
     const dim3 grid(2, CTXT_PARTS * g.H, nq);
     if (full) {

@@ -217,6 +217,8 @@ int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_de
                           s.sec_in.as<uint16_t>(), f->sec_chunk, f->g1, slot_maps(f->ctx, f->g1.log2n), f->ctx->T, st);
   const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
   const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
+  const auto tc = f->tuned_chain.find(nb);
+  const bool clustered = tc != f->tuned_chain.end() && tc->second;
   for (int c0 = 0; c0 < nb; c0 += f->sec_chunk) {
     const int nc = std::min(f->sec_chunk, nb - c0);
     const int nl = CTXT_PARTS * nc;
@@ -228,7 +230,7 @@ int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_de
     launch_encode_rows(f->secE.as<uint32_t>(), f->ws.Ahat.as<uint32_t>(), g2, l_in, nl, f->ctx->T, st);
     launch_encode_lift(f->ws.Ahat.as<uint32_t>(), f->secE.as<uint32_t>(), g2, nl, 1, maps, f->ctx->T, st);
     launch_secondary_chain(f->secE.as<uint32_t>(), s.qbrv.as<uint32_t>() + (size_t)c0 * QV_WORDS_PER_QUERY * n,
-                           QV_WORDS_PER_QUERY * n, nc, f->chain_out.as<uint32_t>(), g2, cc, f->ctx->T, st);
+                           QV_WORDS_PER_QUERY * n, nc, f->chain_out.as<uint32_t>(), g2, cc, f->ctx->T, st, clustered);
     launch_reply(f->chain_out.as<uint32_t>(), nc, g2.H, reply_dev ? reply_dev + (size_t)c0 * reply_stride : nullptr,
                  reply_stride, reply_zq ? reply_zq + (size_t)c0 * CTXT_PARTS * 2 * n : nullptr, g2.log2n, f->ctx->T,
                  st);
@@ -370,6 +372,7 @@ int dnspir_fleet_set_engine(dnspir_fleet* f, int engine) {
   f->tuned.clear();
   f->tuned_cc.clear();
   f->tuned_serial.clear();
+  f->tuned_chain.clear();
   return DNSPIR_OK;
 }
 
@@ -522,13 +525,35 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
       cudaGetLastError();
     }
   }
+  // chain form: the best shape and schedule again with the two-block-cluster
+  // chains at every chunk size (they can share SMs with the next group's scan)
+  bool clustered = false;
+  if (rc == DNSPIR_OK && best_i >= 0) {
+    f->tuned[nb] = best_i;
+    f->tuned_serial[nb] = serial;
+    f->tuned_chain[nb] = 1;
+    rc = dnspir_fleet_process_queries(f, ptrs.data(), lens.data(), (uint32_t)(nb * groups), r.as<uint8_t>(), RB,
+                                      nullptr, 1);
+    if (rc == DNSPIR_OK) {
+      std::lock_guard<std::mutex> lk(f->mu);
+      float t = 0;
+      if (cudaEventElapsedTime(&t, f->tev[6], f->tev[17]) == cudaSuccess && t / 2 < best) {
+        clustered = true;
+        best = t / 2;
+        if (ms_per_shape) ms_per_shape[best_i] = best;
+      }
+      cudaGetLastError();
+    }
+  }
   f->batch = old_batch;
   f->tuned = old_tuned;
   f->tuned_serial.erase(nb);
+  f->tuned_chain.erase(nb);
   if (rc != DNSPIR_OK) return rc;
   if (best_i < 0) return fail(DNSPIR_ERR_CUDA, "no tile shape ran");
   f->tuned[nb] = best_i;
   f->tuned_serial[nb] = serial;
+  f->tuned_chain[nb] = clustered ? 1 : 0;
   if (chosen) *chosen = best_i;
   return DNSPIR_OK;
 }
@@ -593,11 +618,15 @@ int dnspir_fleet_set_schedule(dnspir_fleet* f, uint32_t batch, int schedule) {
   std::lock_guard<std::mutex> lk(f->mu);
   NOT_SERVING(f);
   if (batch < 1 || batch > (uint32_t)TENSOR_MAX_BATCH) return fail(DNSPIR_ERR_BAD_ARG, "batch must be 1..256");
-  if (schedule < -1 || schedule > 2) return fail(DNSPIR_ERR_BAD_ARG, "schedule must be -1, 0, 1 or 2");
-  if (schedule < 0)
+  if (schedule < -1 || schedule > 6 || (schedule >= 0 && (schedule & 3) == 3))
+    return fail(DNSPIR_ERR_BAD_ARG, "schedule must be -1 or 0, 1, 2 plus optionally 4");
+  if (schedule < 0) {
     f->tuned_serial.erase((int)batch);
-  else
-    f->tuned_serial[(int)batch] = schedule;
+    f->tuned_chain.erase((int)batch);
+  } else {
+    f->tuned_serial[(int)batch] = schedule & 3;
+    f->tuned_chain[(int)batch] = schedule >> 2;
+  }
   return DNSPIR_OK;
 }
 

@@ -56,6 +56,7 @@ struct dnspir_fleet {
   dnspir::DBuf qb, err_word, tmp_lane;        // tensor engine: query operand, wait-error word, preprocessing scratch
   std::map<int, int> tuned;                   // tensor engine: group size -> tile shape index
   std::map<int, int> tuned_cc;                // CUDA-core engine: group size -> queries per block
+  std::map<int, int> tuned_chain;             // group size -> 1: two-block-cluster chains at every chunk size
   std::map<int, int> tuned_serial;            // group size -> schedule: 0 the primary phase overlaps the previous
                                               // group's secondary, 1 waits for all of it, 2 waits until it
                                               // reaches its last chunk

@@ -75,7 +75,8 @@ void launch_primary_finalize(const uint32_t* a_out, int nshards, uint64_t* a_zq,
 // vectors [q][slot][p][pos] (bit-reversed), slots 0 gk0, 1 gk1, 2 pq, 3 pqc, 4 sq, 5 sqc.
 // out: [q][h][part][a/b][p][pos].
 void launch_secondary_chain(const uint32_t* E, const uint32_t* qv, size_t qv_stride, int nq, uint32_t* out,
-                            const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st);
+                            const Group& g, const ChainConsts& cc, const NttTables& T, cudaStream_t st,
+                            bool clustered = false);
 
 // ---- primary scan (main_pir_loop, base_pir.rs:1085-1247)
 // B queries (a power of two up to 256) in one launch over all shards, each

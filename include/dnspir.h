@@ -145,7 +145,9 @@ int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, ui
  * milliseconds per group.  The schedule is tuned too: the best shape is timed
  * again with each group's primary phase waiting for the previous group's
  * secondary phase, and again waiting only until that phase starts its last
- * chunk; the fastest of the three schedules is kept for the group size. */
+ * chunk; the fastest of the three schedules is kept for the group size, and
+ * then the two-block-cluster form of the secondary chains is tried at every
+ * chunk size (kept when faster; dnspir_fleet_set_schedule's +4). */
 int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
 /* CUDA-core engine: time the scan of a group of `batch` queries (a power of two
  * up to 256, one launch) with 1, 2, 4, 8 and 16 queries per block and keep the
@@ -155,7 +157,9 @@ int dnspir_fleet_tune_cuda_cores(dnspir_fleet* fleet, uint32_t batch, double* ms
 /* How a group of `batch` queries follows the previous group, overriding the
  * default or a previous tune: 0 its primary phase overlaps the previous
  * group's secondary phase, 1 it waits for all of that phase, 2 it waits until
- * that phase starts its last chunk; -1 returns to the default (0).  Either
+ * that phase starts its last chunk; plus 4: its secondary chains run as
+ * two-block clusters (one RNS factor per block) at every chunk size instead of
+ * one block per part beyond one wave.  -1 returns to the default (0).  Either
  * engine.  No counterpart in the reference. */
 int dnspir_fleet_set_schedule(dnspir_fleet* fleet, uint32_t batch, int schedule);
 /* Tensor engine: use tile shape `shape_index` (dnspir_tscan_shapes order) for

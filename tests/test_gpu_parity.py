@@ -273,12 +273,13 @@ def test_full_secondary_group_matches_oracle(full_secondary, batch, nq):
         assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), (i, j)
 
 
-@pytest.mark.parametrize("schedule", [0, 1, 2])
+@pytest.mark.parametrize("schedule", [0, 1, 2, 6])
 def test_group_schedules_keep_replies(full_secondary, schedule):
     # 64 queries answered as two groups of 32 in one call; each group's
     # secondary phase runs in two chunks (24 + 8 queries), and the second
     # group's primary phase overlaps the first group's secondary phase (0),
-    # waits for all of it (1) or for its last chunk to start (2).  Every reply
+    # waits for all of it (1) or for its last chunk to start (2); 6 is 2 with
+    # the 24-query chunk's chains as two-block clusters.  Every reply
     # decrypts; one per group is compared with the oracle byte for byte.
     data, refs, fleet, l1, l2, count = full_secondary
     rng = orc.Rng(bytes([9, schedule]) + bytes(30))
