@@ -537,6 +537,8 @@ def main():
                 ch, tms, shapes = fleet.tune(B, pipeline=True)
                 shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
                          "persistent": bool(shapes[ch][3]),
+                         "schedule": {"order": ("overlap", "serial", "last chunk")[fleet.get_schedule(B) & 3],
+                                      "cluster_chains": bool(fleet.get_schedule(B) & 4)},
                          "tuned_ms_per_group": round(float(tms[ch]), 3), "tuner": "whole-group pipeline"}
             else:
                 pb, tms = fleet.tune_cuda_cores(B)

@@ -91,6 +91,7 @@ def lib():
         L.dnspir_fleet_scan.argtypes = [_vp, _vp, c.c_uint32, _vp]
         L.dnspir_fleet_set_tile.argtypes = [_vp, c.c_uint32, c.c_int]
         L.dnspir_fleet_set_schedule.argtypes = [_vp, c.c_uint32, c.c_int]
+        L.dnspir_fleet_get_schedule.argtypes = [_vp, c.c_uint32, _vp]
         L.dnspir_fleet_tune_pipeline.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_fleet_tune_cuda_cores.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
@@ -397,6 +398,12 @@ class Fleet:
         start; plus 4 for two-block-cluster chains at every chunk size; -1 the
         default."""
         _check(lib().dnspir_fleet_set_schedule(self._h, batch, schedule))
+
+    def get_schedule(self, batch):
+        """The schedule in force for groups of `batch` (set_schedule's encoding)."""
+        s = ctypes.c_int()
+        _check(lib().dnspir_fleet_get_schedule(self._h, batch, ctypes.byref(s)))
+        return s.value
 
     def set_engine(self, engine):
         """ENGINE_CUDA_CORES or ENGINE_TENSOR; marks every shard unprepared."""

@@ -630,6 +630,15 @@ int dnspir_fleet_set_schedule(dnspir_fleet* f, uint32_t batch, int schedule) {
   return DNSPIR_OK;
 }
 
+int dnspir_fleet_get_schedule(dnspir_fleet* f, uint32_t batch, int* schedule) {
+  if (!f || !schedule) return fail(DNSPIR_ERR_BAD_ARG, "null fleet or output");
+  std::lock_guard<std::mutex> lk(f->mu);
+  const auto so = f->tuned_serial.find((int)batch);
+  const auto tc = f->tuned_chain.find((int)batch);
+  *schedule = (so == f->tuned_serial.end() ? 0 : so->second) + (tc != f->tuned_chain.end() && tc->second ? 4 : 0);
+  return DNSPIR_OK;
+}
+
 int dnspir_fleet_set_tile(dnspir_fleet* f, uint32_t batch, int shape_index) {
   if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
   std::lock_guard<std::mutex> lk(f->mu);

@@ -162,6 +162,10 @@ int dnspir_fleet_tune_cuda_cores(dnspir_fleet* fleet, uint32_t batch, double* ms
  * one block per part beyond one wave.  -1 returns to the default (0).  Either
  * engine.  No counterpart in the reference. */
 int dnspir_fleet_set_schedule(dnspir_fleet* fleet, uint32_t batch, int schedule);
+/* The schedule in force for groups of `batch` queries, in the encoding of
+ * dnspir_fleet_set_schedule (what the pipeline tuner chose, or the default 0).
+ * No counterpart in the reference. */
+int dnspir_fleet_get_schedule(dnspir_fleet* fleet, uint32_t batch, int* schedule);
 /* Tensor engine: use tile shape `shape_index` (dnspir_tscan_shapes order) for
  * groups of `batch` queries, overriding the table or a previous tune; -1
  * returns to the default.  No counterpart in the reference. */

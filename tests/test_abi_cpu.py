@@ -99,6 +99,7 @@ def test_null_handles_are_rejected():
     assert L.dnspir_fleet_tune_cuda_cores(None, 1, None, None) == 6
     assert L.dnspir_fleet_set_tile(None, 1, 0) == 6
     assert L.dnspir_fleet_set_schedule(None, 1, 0) == 6
+    assert L.dnspir_fleet_get_schedule(None, 1, None) == 6
     assert L.dnspir_server_destroy(None) == 0 and L.dnspir_fleet_destroy(None) == 0
 
 

@@ -137,6 +137,7 @@ def test_tensor_tune_pipeline_keeps_replies(config1_pair):
     data, fa, fb, refs, l1, l2, shards = config1_pair
     chosen, ms, shapes = fb.tune(6, pipeline=True)
     assert 0 <= chosen < len(shapes) and ms[chosen] > 0
+    assert fb.get_schedule(6) in (0, 1, 2, 4, 5, 6)
     rng = orc.Rng(bytes([8]) + bytes(31))
     qs = [orc.prepare_query(rng, (97 * k) % 8192, k % shards, l1, l2) for k in range(6)]
     fb.set_batch(6)
