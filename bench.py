@@ -14,16 +14,23 @@ reply.  Every answer is decrypted by the client and compared with the stored
 entry.  The scan runs on the tensor engine (8-bit limb products on tcgen05)
 unless --engine cuda selects the CUDA-core engine; both give the same replies.
 
-After the plain run, the same fleet answers groups of B queries per pass over
-the slabs (--batched, default 16, 64 and 128; tile shape per B from the autotuner):
-responses/s, p50/p99 per-query latency and the scan's effective GB/s
-(B x slab bytes / scan time) go to the "batched" object of the same line.
+After the plain run, on the same fleet:
+  * the reference bench's own 16 (primary, secondary) index pairs
+    (pir_wrapper.rs:562, secondary index j mod S), answered and decrypted;
+  * groups of B queries per pass over the slabs (--batched, default 16, 64,
+    128 and 256; tile shape and schedule per B from the autotuner):
+    responses/s, p50/p99 per-query latency and the scan's effective GB/s
+    (B x slab bytes / scan time) in the "batched" object.
+Then, with the 2^22 fleet released (unless --quick):
+  * "config3" / "config4": 2^20 entries (64 full shards, all resident) on the
+    CUDA-core and on the tensor engine, groups of 16, 64 and 256;
+  * "served": the served mix for a few seconds at 5000 queries/s (below).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--engine tensor|cuda] [--batched 16,64,128]
+                  [--engine tensor|cuda] [--batched 16,64,128,256] [--quick]
   python bench.py --serve [--serve-rate 5000] [--serve-seconds 10]
 
---serve measures the served mix instead: four resident databases (2^15,
+--serve measures the served mix alone: four resident databases (2^15,
 2^18, 2^20 and 2^22 entries; the last on as many distinct shards as fit),
 open-loop Poisson arrivals at the given total rate split by --serve-mix,
 answered by the serving loop (continuous batching, CUDA graphs, half of the
@@ -34,8 +41,9 @@ and p50/p99 submit-to-reply latency per database.
 and answers its own queries (queries are the units; no data-path collective),
 value = all ranks' responses / max-over-ranks device time.
 --impl reference times the CPU restatement of the reference's answer path
-(oracle/, the reference itself is Rust and cannot be built here) on the host
-cores, rank 0 only.
+(oracle/; the reference itself is Rust and cannot be built here) on the host
+cores, rank 0 only: every step is one whole query (all shards scanned, then
+the secondary phase), timed for real.
 """
 import argparse
 import hashlib
@@ -70,12 +78,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--entries", type=int, default=ENTRIES_DEFAULT)
     ap.add_argument("--distinct", type=int, default=0, help="distinct shards in HBM (0 = as many as fit)")
-    ap.add_argument("--cpu-sample-shards", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--engine", default="tensor", choices=["tensor", "cuda"])
-    ap.add_argument("--batched", default="16,64,128", help="comma-separated group sizes measured after the plain run")
+    ap.add_argument("--batched", default="16,64,128,256", help="comma-separated group sizes measured after the plain run")
+    ap.add_argument("--quick", action="store_true", help="skip the 2^20 and served-mix legs")
+    ap.add_argument("--tile", default="", help="B:shape,... force a tensor tile shape for group size B (no tuning)")
+    ap.add_argument("--cpu-distinct", type=int, default=4, help="distinct shard slabs in host RAM for the CPU arm")
     ap.add_argument("--batched-groups", type=int, default=3, help="timed groups per batched size")
-    ap.add_argument("--reserve-gib", type=float, default=22.0, help="HBM left free for workspaces")
+    ap.add_argument("--reserve-gib", type=float, default=0.0, help="HBM left free for workspaces (0: from the group sizes)")
     ap.add_argument("--serve", action="store_true", help="served mix over four databases instead")
     ap.add_argument("--serve-rate", default="5000", help="offered queries/s (comma-separated for several runs)")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
@@ -217,13 +227,12 @@ def group_sizes(cap):
     return sorted(out)
 
 
-def run_serve(args, rank, local_rank):
-    """Served mix (continuous batching over four resident databases)."""
+def serve_mix(args, local_rank, rates, seconds):
+    """The served mix (continuous batching over four resident databases) at
+    each offered rate for `seconds`: (per-rate results, preprocessing s).
+    Raises RuntimeError when a sampled reply fails decryption."""
     import torch
     import dnspir_b200 as dp
-    if rank != 0:
-        return 0
-    torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     sizes = [1 << 15, 1 << 18, 1 << 20, 1 << 22]
     shares = [float(x) for x in args.serve_mix.split(",")]
@@ -266,7 +275,7 @@ def run_serve(args, rank, local_rank):
             pool.append((q, sk, i, j))
         pools.append(pool)
     results = []
-    for rate in [float(r) for r in args.serve_rate.split(",")]:
+    for rate in rates:
         sv = dp.Server(max_sessions=2 * args.serve_clients * len(sizes), device=local_rank)
         ids = [sv.add_db(f, batch_cap[e]) for f, e in zip(fleets, sizes)]
         for i, e in zip(ids, sizes):
@@ -287,7 +296,7 @@ def run_serve(args, rank, local_rank):
                         sv.wait(t, timeout_ms=600000)
         base = [sv.stats(i) for i in ids]
         arrivals = np.random.default_rng(7)
-        n_total = int(rate * args.serve_seconds)
+        n_total = int(rate * seconds)
         gaps = arrivals.exponential(1.0 / rate, size=n_total)
         which = arrivals.choice(len(sizes), size=n_total, p=np.array(shares) / sum(shares))
         clients = arrivals.integers(0, args.serve_clients, size=n_total)
@@ -335,11 +344,30 @@ def run_serve(args, rank, local_rank):
         sv.stop()
         sv.close()
         if bad:
-            print(json.dumps({"error": f"served mix: {bad} of {ok + bad} sampled replies failed decryption"}))
-            return 1
+            for f in fleets:
+                f.close()
+            raise RuntimeError(f"served mix: {bad} of {ok + bad} sampled replies failed decryption")
         results.append({"offered_per_sec": rate, "responses_per_sec": n_total / (t_end - t_start),
                         "submit_seconds": t_submitted - t_start, "drain_seconds": t_end - t_submitted,
                         "per_db": per_db, "checked": {"decrypted_ok": ok, "of": ok + bad}})
+    for f in fleets:
+        f.close()
+    return results, prep_s
+
+
+def run_serve(args, rank, local_rank):
+    """--serve: the served mix alone, one JSON line."""
+    import torch
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    shares = [float(x) for x in args.serve_mix.split(",")]
+    try:
+        results, prep_s = serve_mix(args, local_rank, [float(r) for r in args.serve_rate.split(",")],
+                                    args.serve_seconds)
+    except RuntimeError as e:
+        print(json.dumps({"error": str(e)}), flush=True)
+        return 1
     line = {"metric": "served_mix_responses_per_sec", "value": results[0]["responses_per_sec"],
             "unit": "responses/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
             "config": {"workload": "served mix: Poisson arrivals over four resident databases (2^15, 2^18, 2^20, "
@@ -349,44 +377,82 @@ def run_serve(args, rank, local_rank):
             "runs": results, "preprocess_s": prep_s,
             "latency_note": "submit-to-reply wall time on the host, queueing included"}
     print(json.dumps(line), flush=True)
-    for f in fleets:
-        f.close()
     return 0
 
 
+def workload_config(entries, l1, l2, shards, world):
+    """The workload of the headline line, identical in both arms."""
+    return {
+        "workload": f"plain two-level PIR answer, one query per step, {entries} entries x 2560 B ({shards} shards of "
+                    f"group order {l1}, secondary group order {l2})",
+        "entries": entries, "shards": shards, "primary_order": l1, "secondary_order": l2,
+        "query_bytes": 2 * 2048 * 50 // 8 + (2 if l1 == 2048 else 1) * 2048 * 34 // 8 +
+                       (2 if l2 == 2048 else 1) * 2048 * 34 // 8,
+        "reply_bytes": 22272,
+        "l2": "inputs larger than L2 (each step streams every shard slab: 206 GB at 2^22)",
+        "parallelism": f"replica x{world}" if world > 1 else "single process"}
+
+
+def cpu_query_steps(l1, l2, shards, distinct, warmup, steps):
+    """One whole query per step on the host cores (oracle/scan_baseline.cpp):
+    the AVX-512 main_pir_loop restatement over every logical shard (distinct
+    slabs in RAM, shard k -> k mod distinct) on all threads, then the
+    oracle's secondary phase.  Returns per-step (scan s, secondary s) and the
+    scan's thread count."""
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    orc.set_num_threads(threads)
+    qb = orc.QueryBench(11, l1, l2, shards, min(distinct, shards))
+    try:
+        for _ in range(warmup):
+            qb.step(threads)
+        out, used = [], threads
+        for _ in range(steps):
+            a, b, used = qb.step(threads)
+            out.append((a, b))
+    finally:
+        qb.close()
+    return out, used
+
+
+def cpu_sample_text(l1, l2, shards, distinct, steps, used, scan_s, sec_s):
+    from oracle import oracle as orc
+    return (f"{steps} whole queries timed for real: main_pir_loop restatement (AVX-512 op sequence, "
+            f"{'AVX-512 present' if orc.cpu_has_avx512() else 'NO AVX-512: scalar loop'}) over all {shards} shards "
+            f"({min(distinct, shards)} distinct slabs in host RAM, shard k -> k mod {min(distinct, shards)}) on {used} "
+            f"threads, {scan_s:.2f} s per query, then the scalar oracle's secondary phase (set_db + scan at order "
+            f"{l2}, parallel over the 16 (half, lane) chains), {sec_s:.2f} s per query")
+
+
 def run_reference(args, rank):
-    """CPU restatement of the reference's answer path, timed on the host cores."""
+    """CPU restatement of the reference's answer path, timed on the host cores.
+    Uses the oracle only (the product library is not loaded)."""
     if rank != 0:
         return 0
     from oracle import oracle as orc
-    import dnspir_b200 as dp
-    l1, l2, shards = dp.get_database_shape(args.entries)
-    threads = os.cpu_count() or 1
-    orc.set_num_threads(threads)
-    sample = max(1, min(args.cpu_sample_shards, shards))
-    t_sec = orc.time_secondary(11, l2)
-    for _ in range(args.warmup):
-        orc.scan_baseline(11, l1, sample, threads, 1)
-    per_step = []
-    for _ in range(args.steps):
-        t, used = orc.scan_baseline(11, l1, sample, threads, 1)
-        per_step.append(t * shards / sample + t_sec)
+    world = args.gpus
+    l1, l2, shards = orc.get_database_shape(args.entries)
+    steps, used = cpu_query_steps(l1, l2, shards, args.cpu_distinct, args.warmup, args.steps)
+    per_step = [a + b for a, b in steps]
     total = sum(per_step)
     value = args.steps / total
+    scan_s = statistics.mean(a for a, _ in steps)
+    sec_s = statistics.mean(b for _, b in steps)
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": value * REF_RESPONSE_S_8T, "dtype": "u32",
         "data": "synthetic",
-        "config": {"workload": f"two-level PIR answer, {args.entries} entries x 2560 B, {shards} shards of order {l1}, "
-                               f"secondary order {l2}", "entries": args.entries, "shards": shards},
-        "p50_ms": 1e3 * statistics.median(per_step), "p99_ms": 1e3 * max(per_step),
+        "config": workload_config(args.entries, l1, l2, shards, world),
+        "p50_ms": 1e3 * statistics.median(per_step), "p99_ms": 1e3 * float(np.percentile(per_step, 99)),
+        "primary_ms": 1e3 * scan_s, "secondary_ms": 1e3 * sec_s,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
-                         "avx512": orc.cpu_has_avx512(),
-                         "sample": f"main_pir_loop restatement (AVX-512 op sequence) over {sample} of {shards} shards "
-                                   f"per step scaled x{shards / sample:g}, plus the oracle secondary phase "
-                                   f"(set_db + scan at order {l2}, {t_sec:.2f} s) timed once"},
+                         "avx512": bool(orc.cpu_has_avx512()),
+                         "sample": cpu_sample_text(l1, l2, shards, args.cpu_distinct, args.steps, used, scan_s, sec_s)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "C++ restatement of the reference's answer path (the reference is Rust and cannot be built here); "
+                "the reference's published 2^22 response time is 4.3 s on 8 threads of a Xeon Gold 5318S "
+                "(ARTIFACT-APPENDIX.md:122)",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -394,16 +460,142 @@ def run_reference(args, rank):
 
 def cpu_baseline_line(args, l1, l2, shards):
     from oracle import oracle as orc
-    threads = os.cpu_count() or 1
-    orc.set_num_threads(threads)
-    sample = max(1, min(args.cpu_sample_shards, shards))
-    t_scan, used = orc.scan_baseline(11, l1, sample, threads, 2)
-    t_sec = orc.time_secondary(11, l2)
-    per_query = t_scan * shards / sample + t_sec
-    return {"value": 1.0 / per_query, "unit": UNIT, "cores": used, "kind": "port", "avx512": orc.cpu_has_avx512(),
-            "sample": f"main_pir_loop restatement (AVX-512 op sequence) over {sample} of {shards} shards "
-                      f"({t_scan * 1e3 / sample:.1f} ms/shard) scaled x{shards / sample:g}, plus one oracle secondary "
-                      f"phase at order {l2} ({t_sec:.2f} s)"}
+    steps, used = cpu_query_steps(l1, l2, shards, args.cpu_distinct, 1, 2)
+    per_step = [a + b for a, b in steps]
+    scan_s = statistics.mean(a for a, _ in steps)
+    sec_s = statistics.mean(b for _, b in steps)
+    return {"value": len(per_step) / sum(per_step), "unit": UNIT, "cores": used, "kind": "port",
+            "avx512": bool(orc.cpu_has_avx512()),
+            "sample": cpu_sample_text(l1, l2, shards, args.cpu_distinct, len(per_step), used, scan_s, sec_s)}
+
+
+# the (primary, secondary) index pairs of the reference's bench (pir_wrapper.rs:562)
+REFERENCE_INDICES = [(0, 0), (1, 0), (0, 1), (1, 1), (2, 2), (1, 2), (2, 0), (2, 1), (2, 2), (2742, 128), (923, 255),
+                     (1389, 129), (200, 200), (4000, 255), (3000, 0), (3000, 1)]
+
+
+def fixed_index_leg(dp, torch, fleet, l1, l2, shards, distinct, per_shard_entries, dev, rank):
+    """The reference bench's 16 index pairs, one query per call through the
+    host path, each reply decrypted and compared with the stored entry."""
+    ok, times = 0, []
+    for k, (i, j) in enumerate(REFERENCE_INDICES):
+        q, sk = dp.prepare_query(hashlib.sha256(f"fixed-{rank}-{k}".encode()).digest(), i, j % shards, l1, l2)
+        t0 = time.perf_counter()
+        r = fleet.process_query(q)
+        times.append(1e3 * (time.perf_counter() - t0))
+        want = pack_host(shard_payload(torch, (j % shards) % distinct, per_shard_entries, dev)[i].cpu().numpy().tobytes())
+        ok += int(np.array_equal(dp.process_reply(r, sk), want))
+    return {"pairs": "pir_wrapper.rs:562, secondary index j mod S", "of": len(REFERENCE_INDICES), "decrypted_ok": ok,
+            "p50_ms": statistics.median(times), "max_ms": max(times),
+            "note": "host buffers, one query per call (copies and host staging included)"}
+
+
+def batched_leg(dp, torch, dev, entries, engine, sizes, groups, check_every=8):
+    """BASELINE configs 3 and 4: a database of `entries` entries with every
+    shard resident, groups of B queries per pass on one engine; responses/s,
+    per-query p50/p99, scan and secondary time per group, decryption of a
+    sample of every group size."""
+    l1, l2, shards = dp.get_database_shape(entries)
+    per = 8 * l1
+    slab_bytes = dp.required_memory_general(11, l1) * 32
+    t0 = time.time()
+    fleet = dp.Fleet(entries, shards)
+    if engine == "tensor":
+        fleet.set_engine(dp.ENGINE_TENSOR)
+    for first in range(0, shards, 8):
+        cnt = min(8, shards - first)
+        co = torch.empty((cnt, per, dp.N), dtype=torch.uint16, device=dev)
+        for i in range(cnt):
+            dp.pack_payloads(shard_payload(torch, first + i, per, dev, seed0=3000), co[i], device=dev.index or 0)
+        fleet.set_shards(first, co)
+        del co
+    torch.cuda.synchronize()
+    prep_s = time.time() - t0
+    stream = torch.cuda.current_stream()
+    fleet.set_stream(stream.cuda_stream)
+    rng = np.random.default_rng(20)
+    pool_n = 2 * max(sizes)
+    pidx = [(int(rng.integers(0, per)), int(rng.integers(0, shards))) for _ in range(pool_n)]
+    pq, pseeds = [], []
+    for k, (i, j) in enumerate(pidx):
+        q, sk = dp.prepare_query(hashlib.sha256(f"c34-{engine}-{k}".encode()).digest(), i, j, l1, l2)
+        pq.append(q)
+        pseeds.append(sk)
+    qlen = len(pq[0])
+    pdev = torch.tensor(np.frombuffer(b"".join(pq), dtype=np.uint8).reshape(pool_n, qlen), device=dev)
+    out = {"entries": entries, "shards": shards, "primary_order": l1, "secondary_order": l2,
+           "resident": f"all {shards} shards ({shards * slab_bytes / 2**30:.0f} GiB)", "engine": engine,
+           "preprocess_s": prep_s, "groups": {}}
+    for B in sizes:
+        if engine == "tensor":
+            ch, tms, shapes = fleet.tune(B, pipeline=True)
+            tile = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
+                    "persistent": bool(shapes[ch][3]), "schedule": fleet.get_schedule(B)}
+        else:
+            pb, _ = fleet.tune_cuda_cores(B)
+            tile = {"queries_per_block": pb}
+        fleet.set_batch(B)
+        nq = B * groups
+        sel = torch.arange(nq, device=dev) % pool_n
+        qin = pdev[sel].contiguous()
+        rout = torch.zeros((nq, dp.reply_bytes()), dtype=torch.uint8, device=dev)
+        fleet.process_queries_device(qin[:2 * B], rout[:2 * B])  # warm-up: both buffer slots
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fleet.process_queries_device(qin, rout)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        bt = fleet.batch_timings(nq)
+        host = rout.cpu().numpy()
+        check = list(range(0, nq, max(1, nq // check_every)))
+        good = 0
+        for k in check:
+            i, j = pidx[k % pool_n]
+            want = pack_host(shard_payload(torch, j, per, dev, seed0=3000)[i].cpu().numpy().tobytes())
+            good += int(np.array_equal(dp.process_reply(host[k].tobytes(), pseeds[k % pool_n]), want))
+        scan = statistics.mean(float(bt[3, g * B]) for g in range(groups))
+        out["groups"][str(B)] = {
+            "responses_per_sec": nq / (ms * 1e-3), "p50_ms": float(np.median(bt[0])),
+            "p99_ms": float(np.percentile(bt[0], 99)), "scan_ms_per_group": scan,
+            "secondary_ms_per_group": statistics.mean(float(bt[2, g * B]) for g in range(groups)),
+            "scan_hbm_gbs": shards * slab_bytes / (scan * 1e-3) / 1e9,
+            "scan_tensor_pops": (16 * 2 * B * shards * (slab_bytes // 4) / (scan * 1e-3) / 1e15
+                                 if engine == "tensor" else None),
+            "tile": tile, "checked": {"decrypted_ok": good, "of": len(check)}}
+        del qin, rout
+        if good != len(check):
+            fleet.close()
+            raise RuntimeError(f"{entries} entries, {engine}, B={B}: {len(check) - good} answers failed")
+    fleet.set_batch(1)
+    fleet.close()
+    del pdev
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def extra_legs(args, dp, torch, dev, local_rank):
+    """BASELINE configs 3, 4 (2^20, both engines) and 5 (served mix), run
+    after the 2^22 fleet is released."""
+    legs = {}
+    try:
+        legs["config3"] = batched_leg(dp, torch, dev, 1 << 20, "cuda", [16, 64, 256], 2)
+        legs["config3"]["note"] = ("CUDA-core modular-MAC scan (u32 x u32 -> u64), one launch per group; the reference "
+                                   "rule gives full shards at 2^20 (pir_wrapper.rs:188, 223-227)")
+        legs["config4"] = batched_leg(dp, torch, dev, 1 << 20, "tensor", [16, 64, 256], 3)
+        legs["config4"]["note"] = ("INT8 limb products on tcgen05 (u8 x u8 -> s32, 16 limb products per residue "
+                                   "product, K <= 6144 so no partial sum overflows), recombined and reduced mod each "
+                                   "prime; scan_tensor_pops counts int8 limb operations (2 per MAC)")
+        results, prep_s = serve_mix(args, local_rank, [5000.0], 3.0)
+        legs["served"] = {"offered_per_sec": 5000.0, "seconds": 3.0, "preprocess_s": prep_s,
+                          "mix": [float(x) for x in args.serve_mix.split(",")], **results[0],
+                          "latency_note": "submit-to-reply wall time on the host, queueing included"}
+    except RuntimeError as e:
+        return {"error": str(e)}
+    return legs
 
 
 def main():
@@ -427,7 +619,12 @@ def main():
     per_shard_entries = 8 * l1
     slab_bytes = dp.required_memory_general(11, l1) * 32
     free, _ = torch.cuda.mem_get_info()
-    fit = int((free - int(args.reserve_gib * (1 << 30))) // slab_bytes)
+    sizes = [int(x) for x in args.batched.split(",") if x.strip()]
+    # workspaces: two buffer slots of scan output for the largest group, the
+    # secondary phase's chunk (at most 6 GiB) and headroom
+    reserve = args.reserve_gib * (1 << 30) if args.reserve_gib > 0 else \
+        2 * max(sizes + [1]) * shards * 2 * dp.N * 8 * 4 + (14 << 30)
+    fit = int((free - int(reserve)) // slab_bytes)
     distinct = args.distinct if args.distinct > 0 else max(1, min(shards, fit))
 
     # ---- build and preprocess the fleet on the GPU
@@ -481,9 +678,11 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     w0 = args.warmup
+    launches0 = fleet.launch_count()
     ev0.record(stream)
     fleet.process_queries_device(qdev[w0:w0 + args.steps], rdev[w0:w0 + args.steps])
     ev1.record(stream)
+    launches = fleet.launch_count() - launches0
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -516,9 +715,16 @@ def main():
               flush=True)
         return 1
 
+    # ---- the reference bench's own index list (pir_wrapper.rs:562), secondary
+    # index j mod S, answered one query at a time through the host path
+    fixed = fixed_index_leg(dp, torch, fleet, l1, l2, shards, distinct, per_shard_entries, dev, rank)
+    if fixed["decrypted_ok"] != fixed["of"]:
+        print(json.dumps({"error": f"fixed index list: {fixed['of'] - fixed['decrypted_ok']} answers failed"}),
+              flush=True)
+        return 1
+
     # ---- batched: groups of B queries per pass over the slabs, same fleet
     batched = {}
-    sizes = [int(x) for x in args.batched.split(",") if x.strip()]
     if args.engine == "cuda":
         sizes = [b for b in sizes if b <= 256 and b & (b - 1) == 0]
     if sizes:
@@ -531,9 +737,15 @@ def main():
             pq.append(q)
             pseeds.append(sk)
         pdev = torch.tensor(np.frombuffer(b"".join(pq), dtype=np.uint8).reshape(pool_n, qlen), device=dev)
+        forced = {int(a): int(b) for a, b in (x.split(":") for x in args.tile.split(",") if x.strip())}
         for B in sizes:
             shape = None
-            if args.engine == "tensor":
+            if args.engine == "tensor" and B in forced:
+                fleet.set_tile(B, forced[B])
+                sh = dp.tscan_shapes()[forced[B]]
+                shape = {"rows_per_cta": sh[0], "mtiles_per_cta": sh[1], "stages": sh[2], "persistent": bool(sh[3]),
+                         "tuner": "forced (--tile)"}
+            elif args.engine == "tensor":
                 ch, tms, shapes = fleet.tune(B, pipeline=True)
                 shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
                          "persistent": bool(shapes[ch][3]),
@@ -573,6 +785,8 @@ def main():
                 return 1
             gscan = [float(bt[3, g * B]) for g in range(args.batched_groups)]
             batched[str(B)] = {
+                "scan_tensor_pops": (16 * 2 * B * shards * (slab_bytes // 4) / (statistics.mean(gscan) * 1e-3) / 1e15
+                                     if args.engine == "tensor" else None),
                 "responses_per_sec": whole_job_rate(nq, world, bms * 1e-3), "groups": args.batched_groups,
                 "p50_ms": float(np.median(bt[0])), "p99_ms": float(np.percentile(bt[0], 99)),
                 "scan_ms_per_group": statistics.mean(gscan),
@@ -581,6 +795,7 @@ def main():
                 "tile": shape, "checked": {"decrypted_ok": good, "of": len(check)}}
         fleet.set_batch(1)
         fleet.set_stream(None)
+        del pdev, qin, rout
 
     # ---- report
     scan_ms = [p[2] for p in phase]
@@ -591,20 +806,27 @@ def main():
     kname = "tscan_kernel" if args.engine == "tensor" else "scan_batch_kernel"
     traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_batch_2p22.md")
     value = whole_job_rate(args.steps, world, total_ms * 1e-3)
+    fleet.close()
+    del qdev, rdev
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    legs = {}
+    if not args.quick and world == 1:
+        legs = extra_legs(args, dp, torch, dev, local_rank)
+        if "error" in legs:
+            print(json.dumps({"error": legs["error"]}), flush=True)
+            return 1
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value * REF_RESPONSE_S_8T,
         "vs_baseline_ref": "reference response time 4.3 s at 2^22, 8 threads, Xeon Gold 5318S (ARTIFACT-APPENDIX.md:122)",
         "dtype": "u32", "data": "synthetic",
-        "config": {
-            "workload": "plain two-level PIR answer, one query per launch sequence (consecutive queries overlap "
-                        "secondary and primary phases), 2^22 entries x 2560 B "
-                        f"({shards} full shards of 768 MiB, {distinct} distinct resident, shard k -> k mod {distinct})",
-            "entries": args.entries, "shards": shards, "distinct": distinct, "primary_order": l1,
-            "secondary_order": l2, "query_bytes": qlen, "reply_bytes": dp.reply_bytes(),
-            "l2": "inputs larger than L2 (each step streams 206 GB of shard slabs)",
-            "parallelism": f"replica x{world}" if world > 1 else "single GPU"},
+        "config": workload_config(args.entries, l1, l2, shards, world),
+        "distinct_resident": distinct,
+        "resident_note": f"{distinct} distinct full shards resident in HBM, logical shard k served by k mod {distinct} "
+                         "(the reference's --preprocessed-db-count, pir_wrapper.rs:578); consecutive queries overlap "
+                         "the secondary phase of one with the primary phase of the next",
         "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
         "latency_note": "p50/p99: per-query device latency (copy-in to reply) with queries back to back",
         "unloaded_p50_ms": statistics.median(unloaded) if unloaded else None,
@@ -618,15 +840,18 @@ def main():
                      "traffic": traffic, "algorithmic_bytes": algo_bytes},
         "e2e": {"value": whole_job_rate(args.steps, world, e2e_s), "unit": UNIT, "h2d_bytes_per_step": qlen,
                 "d2h_bytes_per_step": dp.reply_bytes()},
-        "gpu_launches": (9 if args.engine == "tensor" else 8) * args.steps,
+        "gpu_launches": launches,
+        "gpu_launches_note": "kernels the library launched in the timed region, counted at each launch "
+                             "(dnspir_fleet_launch_count)",
+        "fixed_indices": fixed,
         "clocks": clk,
         "checked": {"decrypted_ok": ok, "of": args.steps},
     }
+    line.update(legs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_line(args, l1, l2, shards)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    fleet.close()
     if pg:
         pg.destroy_process_group()
     return 0

@@ -20,7 +20,7 @@ import numpy as np
 
 __all__ = [
     "DnspirError", "lib", "get_database_shape", "num_databases", "required_memory_general",
-    "choose_secondary_order", "expand_seed", "query_bytes", "prepare_query", "process_reply", "reply_bytes", "PIRDatabase", "Fleet", "pack_payloads",
+    "choose_secondary_order", "expand_seed", "set_a_parts", "get_a_parts", "load_a_parts_file", "query_bytes", "prepare_query", "process_reply", "reply_bytes", "PIRDatabase", "Fleet", "pack_payloads",
     "LOG2_N", "N", "Q1", "Q2", "Q", "SIMD_COUNT", "PLAIN_MODULUS",
 ]
 
@@ -78,6 +78,8 @@ def lib():
                                                   c.c_uint32, c.POINTER(_vp)]
         L.dnspir_fleet_set_shards.argtypes = [_vp, c.c_uint32, c.c_uint32, _vp, c.c_int]
         L.dnspir_expand_seed.argtypes = [c.c_uint32, c.c_int, _vp]
+        L.dnspir_set_a_parts.argtypes = [c.c_uint32, _vp]
+        L.dnspir_get_a_parts.argtypes = [c.c_uint32, _vp]
         L.dnspir_pack_payloads.argtypes = [c.c_int, _vp, c.c_uint64, _vp]
         L.dnspir_fleet_process_queries.argtypes = [_vp, _vp, _vp, c.c_uint32, _vp, c.c_uint64, _vp, c.c_int]
         L.dnspir_fleet_process_query.argtypes = [_vp, _vp, c.c_uint64, _vp, _u64p]
@@ -94,6 +96,7 @@ def lib():
         L.dnspir_fleet_get_schedule.argtypes = [_vp, c.c_uint32, _vp]
         L.dnspir_fleet_tune_pipeline.argtypes = [_vp, c.c_uint32, _vp, _vp]
         L.dnspir_fleet_tune_cuda_cores.argtypes = [_vp, c.c_uint32, _vp, _vp]
+        L.dnspir_fleet_set_wait_limit.argtypes = [_vp, c.c_uint64, c.c_int]
         L.dnspir_server_create.argtypes = [c.c_int, c.c_uint32, c.POINTER(_vp)]
         L.dnspir_server_add_db.argtypes = [_vp, _vp, c.c_uint32, _u32p]
         L.dnspir_server_start.argtypes = [_vp, c.c_int]
@@ -107,6 +110,7 @@ def lib():
         L.dnspir_server_stop.argtypes = [_vp]
         L.dnspir_server_destroy.argtypes = [_vp]
         L.dnspir_fleet_batch_timings.argtypes = [_vp, c.c_uint32] + [_vp] * 4
+        L.dnspir_fleet_launch_count.argtypes = [_vp, _u64p]
         L.dnspir_fleet_slab_bytes.restype = c.c_uint64
         L.dnspir_fleet_slab_bytes.argtypes = [_vp]
         L.dnspir_fleet_destroy.argtypes = [_vp]
@@ -170,6 +174,37 @@ def expand_seed(log2_n, which):
     out = np.zeros(1 << log2_n, dtype=np.uint64)
     _check(lib().dnspir_expand_seed(log2_n, which, _ptr(out)))
     return out
+
+
+def set_a_parts(log2_n, parts):
+    """Install the six a-parts of ring dimension 2^log2_n process-wide
+    ((6, N) coefficients in [0, q): gk0, gk1, FirstSet query and conjugate,
+    SecondSet query and conjugate -- bfv.rs:46-49, base_pir.rs:104-107), or
+    restore the seed expansion with parts=None.  Shards preprocessed before
+    must be set again."""
+    if parts is None:
+        _check(lib().dnspir_set_a_parts(log2_n, None))
+        return
+    a = np.ascontiguousarray(parts, dtype=np.uint64)
+    assert a.shape == (6, 1 << log2_n)
+    _check(lib().dnspir_set_a_parts(log2_n, _ptr(a)))
+
+
+def get_a_parts(log2_n):
+    """The six a-parts in effect, (6, N) uint64."""
+    out = np.zeros((6, 1 << log2_n), dtype=np.uint64)
+    _check(lib().dnspir_get_a_parts(log2_n, _ptr(out)))
+    return out
+
+
+def load_a_parts_file(path, log2_n=LOG2_N):
+    """Install a-parts from a file: a .npy array of shape (6, N), or raw
+    little-endian uint64 (6 x N values)."""
+    if str(path).endswith(".npy"):
+        parts = np.load(path)
+    else:
+        parts = np.fromfile(path, dtype="<u8").reshape(6, 1 << log2_n)
+    set_a_parts(log2_n, parts)
 
 
 def pack_payloads(payload, out, device=0):
@@ -405,6 +440,11 @@ class Fleet:
         _check(lib().dnspir_fleet_get_schedule(self._h, batch, ctypes.byref(s)))
         return s.value
 
+    def set_wait_limit(self, wait_ns=0, withhold_chunk=-1):
+        """Tensor engine: limit of the scan's pipeline waits (0: default 2 s);
+        withhold_chunk >= 0 is the timeout path's test hook."""
+        _check(lib().dnspir_fleet_set_wait_limit(self._h, wait_ns, withhold_chunk))
+
     def set_engine(self, engine):
         """ENGINE_CUDA_CORES or ENGINE_TENSOR; marks every shard unprepared."""
         _check(lib().dnspir_fleet_set_engine(self._h, engine))
@@ -431,6 +471,12 @@ class Fleet:
 
     def set_stream(self, stream_handle):
         _check(lib().dnspir_fleet_set_stream(self._h, _vp(stream_handle) if stream_handle else None))
+
+    def launch_count(self):
+        """Kernels the answer pipeline has launched so far."""
+        v = ctypes.c_uint64()
+        _check(lib().dnspir_fleet_launch_count(self._h, ctypes.byref(v)))
+        return v.value
 
     @property
     def slab_bytes(self):

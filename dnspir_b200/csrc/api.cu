@@ -126,7 +126,7 @@ struct ChaCha12 {
 
 void expand(uint32_t n, const uint8_t* seed, uint64_t* out) {
   ChaCha12 r(seed);
-  const uint64_t mask = (1ull << 51) - 1;
+  const uint64_t mask = (1ull << 51) - 1;  // ceil(log2 q) = 51 bits
   for (uint32_t i = 0; i < n; i++) {
     uint64_t x;
     do x = r.next_u64() & mask;
@@ -134,7 +134,32 @@ void expand(uint32_t n, const uint8_t* seed, uint64_t* out) {
     out[i] = x;
   }
 }
+
+// The six a-parts in effect per ring dimension: the seed expansion above, or
+// polynomials installed by dnspir_set_a_parts.  `version` changes with every
+// installation, so shards preprocessed under other a-parts can be recognised.
+std::mutex g_ap_mu;
+std::vector<uint64_t> g_ap_override[LOG2_N_MAX + 1];
+uint64_t g_ap_version[LOG2_N_MAX + 1];
 }  // namespace
+
+uint64_t a_parts_version(int log2n) {
+  std::lock_guard<std::mutex> lk(g_ap_mu);
+  return g_ap_version[log2n];
+}
+
+void a_parts_host(int log2n, uint64_t* out, uint64_t* version) {
+  const uint32_t n = 1u << log2n;
+  {
+    std::lock_guard<std::mutex> lk(g_ap_mu);
+    if (version) *version = g_ap_version[log2n];
+    if (!g_ap_override[log2n].empty()) {
+      memcpy(out, g_ap_override[log2n].data(), (size_t)6 * n * 8);
+      return;
+    }
+  }
+  for (int s = 0; s < 6; s++) expand(n, SEEDS[s], out + (size_t)s * n);
+}
 
 // ------------------------------------------------------------ device context
 static std::mutex g_ctx_mu;
@@ -201,21 +226,37 @@ int get_ctx(int device, DeviceCtx** out) {
 }
 
 // a-parts and the sigma_5 position map for ring dimension 2^log2n
-int ctx_consts(DeviceCtx* c, int log2n) {
-  std::lock_guard<std::mutex> lk(c->mu);
-  if (c->consts[log2n]) return DNSPIR_OK;
+// a-parts in NTT form for the a-parts now in effect (rebuilt after
+// dnspir_set_a_parts; earlier buffers are kept, a kernel queued before the
+// change may still read them)
+static int ctx_a_parts(DeviceCtx* c, int log2n, uint64_t* version) {
   const uint32_t n = 1u << log2n;
+  uint64_t ver = 0;
   std::vector<uint64_t> ap(6 * (size_t)n);
-  for (int s = 0; s < 6; s++) expand(n, SEEDS[s], ap.data() + (size_t)s * n);
+  a_parts_host(log2n, ap.data(), &ver);
+  if (version) *version = ver;
+  if (c->consts[log2n] && c->consts_ver[log2n] == ver) return DNSPIR_OK;
   uint64_t* dz = nullptr;
   uint32_t* dc = nullptr;
-  uint32_t* dg = nullptr;
   CK(cudaMalloc(&dz, ap.size() * 8));
   CK(cudaMalloc(&dc, (size_t)6 * 2 * n * 4));
-  CK(cudaMalloc(&dg, (size_t)n * 4));
   CK(cudaMemcpy(dz, ap.data(), ap.size() * 8, cudaMemcpyHostToDevice));
   launch_ring_to_ntt(dz, 6, nullptr, dc, log2n, c->T, 0);
   CK(cudaGetLastError());
+  CK(cudaDeviceSynchronize());
+  CK(cudaFree(dz));
+  if (c->consts[log2n]) c->retired.push_back(c->consts[log2n]);
+  c->consts[log2n] = dc;
+  c->consts_ver[log2n] = ver;
+  return DNSPIR_OK;
+}
+
+int ctx_consts(DeviceCtx* c, int log2n, uint64_t* version) {
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (c->galb[log2n]) return ctx_a_parts(c, log2n, version);
+  const uint32_t n = 1u << log2n;
+  uint32_t* dg = nullptr;
+  CK(cudaMalloc(&dg, (size_t)n * 4));
   std::vector<uint32_t> gb(n);
   const uint32_t two_n = 2 * n;
   uint32_t inv5 = 1;
@@ -246,12 +287,10 @@ int ctx_consts(DeviceCtx* c, int log2n) {
     c->uof[log2n] = duo;
   }
   CK(cudaDeviceSynchronize());
-  CK(cudaFree(dz));
   device_pow5(log2n, false);
   device_pow5(log2n, true);
   c->galb[log2n] = dg;
-  c->consts[log2n] = dc;
-  return DNSPIR_OK;
+  return ctx_a_parts(c, log2n, version);
 }
 
 SlotMaps slot_maps(DeviceCtx* c, int log2n) {
@@ -318,26 +357,55 @@ struct dnspir_db {
   Group g;
   int used_seeds = 0;
   bool ready = false;
+  uint64_t ap_ver = 0;  // a-parts version the slab was preprocessed under
   cudaStream_t st = nullptr;
+  cudaEvent_t noalloc_done = nullptr;  // recorded on the caller's stream after each no-allocation call
   uint32_t* slab = nullptr;
   DBuf a_zq, a_ms, qz, qlane, part, out, slab_ptr;
   EncodeWs ws;
   std::mutex mu;
   ~dnspir_db() {
+    if (noalloc_done) cudaEventDestroy(noalloc_done);
     if (slab) cudaFree(slab);
     if (st) cudaStreamDestroy(st);
   }
 };
 
-// Read-only view of a shard for the no-allocation entry point (noalloc.cu).
 namespace dnspir {
-int db_view(const dnspir_db* db, DbView* out) {
+int noalloc_reserve(int device);  // noalloc.cu
+
+static int db_ready(const dnspir_db* db) {
+  if (!db->ready) return fail(DNSPIR_ERR_NOT_READY, "database not preprocessed");
+  if (db->ap_ver != a_parts_version(db->g.log2n))
+    return fail(DNSPIR_ERR_NOT_READY, "the a-parts changed since the database was preprocessed: call set_db again");
+  return DNSPIR_OK;
+}
+
+// The no-allocation entry point (noalloc.cu) holds the shard's lock from the
+// view until its work is queued; the event recorded on its stream lets set_db
+// and destroy wait for that work before they touch the slab.
+int db_noalloc_begin(dnspir_db* db, DbView* out) {
+  db->mu.lock();
+  const int rc = db_ready(db);
+  if (rc != DNSPIR_OK) {
+    db->mu.unlock();
+    return rc;
+  }
   out->device = db->device;
   out->ready = db->ready;
   out->g = db->g;
   out->slab = db->slab;
   out->T = db->ctx->T;
   out->maps = slot_maps(db->ctx, db->g.log2n);
+  return DNSPIR_OK;
+}
+int db_noalloc_end(dnspir_db* db, cudaStream_t st) {
+  const cudaError_t e = cudaEventRecord(db->noalloc_done, st);
+  db->mu.unlock();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DNSPIR_ERR_CUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
+  }
   return DNSPIR_OK;
 }
 void set_last_error(const std::string& msg) { g_err = msg; }
@@ -392,6 +460,23 @@ int dnspir_expand_seed(uint32_t log2_n, int which, uint64_t* out) {
   return DNSPIR_OK;
 }
 
+int dnspir_set_a_parts(uint32_t log2_n, const uint64_t* coeffs) {
+  if (log2_n < 3 || log2_n > LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_ARG, "log2_n must be in [3, 11]");
+  const size_t n = (size_t)1 << log2_n;
+  if (coeffs && !reduced(coeffs, 6 * n)) return fail(DNSPIR_ERR_BAD_ARG, "a-part coefficients must be below q");
+  std::lock_guard<std::mutex> lk(g_ap_mu);
+  if (coeffs) g_ap_override[log2_n].assign(coeffs, coeffs + 6 * n);
+  else g_ap_override[log2_n].clear();
+  g_ap_version[log2_n]++;
+  return DNSPIR_OK;
+}
+
+int dnspir_get_a_parts(uint32_t log2_n, uint64_t* out) {
+  if (!out || log2_n < 3 || log2_n > LOG2_N_MAX) return fail(DNSPIR_ERR_BAD_ARG, "bad argument");
+  a_parts_host((int)log2_n, out, nullptr);
+  return DNSPIR_OK;
+}
+
 int dnspir_pack_payloads(int device, const uint8_t* bytes, uint64_t entries, uint16_t* coeffs) {
   if (!bytes || !coeffs) return fail(DNSPIR_ERR_BAD_ARG, "null buffer");
   DeviceCtx* c = nullptr;
@@ -419,6 +504,10 @@ int dnspir_db_create(int device, uint32_t log2_n, uint32_t group_order, int used
   d->g = make_group(log2_n, group_order);
   d->used_seeds = used_seeds;
   CK(cudaStreamCreateWithFlags(&d->st, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&d->noalloc_done, cudaEventDisableTiming));
+  // the no-allocation entry point's static region is loaded now, before the
+  // slab takes the memory (module loading is lazy)
+  CKR(noalloc_reserve(device));
   CK(cudaMalloc(&d->slab, slab_words(d->g) * 4));
   CKR(d->a_zq.ensure((size_t)SIMD * d->g.n * 8));
   CKR(d->a_ms.ensure((size_t)SIMD * d->g.n * 4));
@@ -440,8 +529,13 @@ int dnspir_db_set_db(dnspir_db* db, const uint16_t* entries, uint64_t count, int
   }
   uint32_t* slabs[1] = {db->slab};
   db->ready = false;
+  // a no-allocation call queued on another stream may still read the slab
+  CK(cudaStreamWaitEvent(db->st, db->noalloc_done, 0));
+  uint64_t ver = 0;
+  CKR(ctx_consts(db->ctx, db->g.log2n, &ver));
   CKR(preprocess_shards(db->ctx, db->g, db->used_seeds, slabs, 1, src, db->a_zq.as<uint64_t>(),
                         db->a_ms.as<uint32_t>(), db->ws, db->st));
+  db->ap_ver = ver;
   db->ready = true;
   return DNSPIR_OK;
 }
@@ -449,7 +543,7 @@ int dnspir_db_set_db(dnspir_db* db, const uint16_t* entries, uint64_t count, int
 int dnspir_db_get_a(dnspir_db* db, uint64_t* out) {
   if (!db || !out) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(db->mu);
-  if (!db->ready) return fail(DNSPIR_ERR_NOT_READY, "database not preprocessed");
+  CKR(db_ready(db));
   DeviceGuard dg(db->device);
   CK(cudaMemcpy(out, db->a_zq.p, (size_t)SIMD * db->g.n * 8, cudaMemcpyDeviceToHost));
   return DNSPIR_OK;
@@ -459,7 +553,7 @@ int dnspir_db_perform_pir_split(dnspir_db* db, const uint64_t* qry_b, const uint
                                 uint64_t* out_b) {
   if (!db || !qry_b || !gk_b || !out_b) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
   std::lock_guard<std::mutex> lk(db->mu);
-  if (!db->ready) return fail(DNSPIR_ERR_NOT_READY, "database not preprocessed");
+  CKR(db_ready(db));
   const Group& g = db->g;
   if ((g.H == 2) != (qry_conj_b != nullptr))
     return fail(DNSPIR_ERR_BAD_SHAPE, "conjugate query must be given exactly when the group requires it");
@@ -494,6 +588,11 @@ int dnspir_db_perform_pir_split(dnspir_db* db, const uint64_t* qry_b, const uint
 int dnspir_db_destroy(dnspir_db* db) {
   if (!db) return DNSPIR_OK;
   DeviceGuard dg(db->device);
+  {
+    // no-allocation calls still queued on the caller's stream read the slab
+    std::lock_guard<std::mutex> lk(db->mu);
+    cudaEventSynchronize(db->noalloc_done);
+  }
   delete db;
   return DNSPIR_OK;
 }

@@ -139,10 +139,11 @@ P mul_sk(const P& a, const std::vector<int8_t>& sk) {
   return out;
 }
 
+// a-part `which` in effect (the seed expansion, or what dnspir_set_a_parts installed)
 P apart(int which) {
-  std::vector<uint64_t> v(CN);
-  dnspir_expand_seed(11, which, v.data());
-  return P(v.begin(), v.end());
+  std::vector<uint64_t> v((size_t)6 * CN);
+  dnspir_get_a_parts(11, v.data());
+  return P(v.begin() + (size_t)which * CN, v.begin() + (size_t)(which + 1) * CN);
 }
 
 P enc_sym_b(const P& a, Rng& r, const std::vector<int8_t>& sk, const P& m) {  // bfv.rs:72-87

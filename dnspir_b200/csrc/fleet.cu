@@ -110,8 +110,10 @@ int launch_scan(dnspir_fleet* f, QSlot& s, int nb, int Bk) {
     const TScanShape& shape = tensor_shape(f, nb, &nb_pad);
     if (nb_pad != Bk) return fail(DNSPIR_ERR_BAD_ARG, "tensor scan batch mismatch");
     if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), qv, nb, Bk, f->qb.as<uint8_t>(),
-                     s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), shape, f->st))
+                     s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), shape, f->st,
+                     f->limits))
       return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
+    f->launches += 2;  // query operand + scan
     return DNSPIR_OK;
   }
   if (Bk > nb)  // unused query positions of the kernel batch compute on zeros
@@ -121,6 +123,7 @@ int launch_scan(dnspir_fleet* f, QSlot& s, int nb, int Bk) {
   if (launch_scan_batch(f->slabs_dev.as<uint32_t*>(), f->S, s.qnat.as<uint32_t>(), qv, Bk, per_block,
                         s.fin.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), f->st))
     return fail(DNSPIR_ERR_BAD_ARG, "unsupported scan batch");
+  f->launches += 1;
   return DNSPIR_OK;
 }
 
@@ -131,6 +134,8 @@ namespace dnspir {
 int fleet_ready(dnspir_fleet* f) {
   for (uint32_t d = 0; d < f->D; d++)
     if (!f->ready[d]) return fail(DNSPIR_ERR_NOT_READY, "fleet shard not preprocessed");
+  if (f->ap_ver != a_parts_version(f->g1.log2n))
+    return fail(DNSPIR_ERR_NOT_READY, "the a-parts changed since the shards were preprocessed: set the shards again");
   return DNSPIR_OK;
 }
 
@@ -193,10 +198,12 @@ int fleet_primary_kernels(dnspir_fleet* f, QSlot& s, int nb, int Bk, const uint3
                           const uint32_t* sess_brv, cudaEvent_t scan0, cudaEvent_t scan1) {
   const Group& g1 = f->g1;
   const size_t qv = QV_WORDS_PER_QUERY * g1.n;
-  if (s.qbytes.p)
+  if (s.qbytes.p) {
     launch_decode_query(s.qbytes.as<uint8_t>(), s.qdesc.as<QDesc>(), nb, fleet_wire_spec(f), fleet_gk_bytes(f),
                         s.qnat.as<uint32_t>(), s.qbrv.as<uint32_t>(), qv, sess_nat, sess_brv, g1.log2n, f->ctx->T,
                         f->st);
+    f->launches += 1;
+  }
   if (scan0) CK(cudaEventRecord(scan0, f->st));
   CKR(launch_scan(f, s, nb, Bk));
   if (scan1) CK(cudaEventRecord(scan1, f->st));
@@ -215,6 +222,7 @@ int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_de
   // reads and writes only this slot's buffers
   launch_primary_epilogue(s.fin.as<uint32_t>(), nb, f->S, f->a_ms.as<uint32_t>(), f->distinct_dev.as<int>(),
                           s.sec_in.as<uint16_t>(), f->sec_chunk, f->g1, slot_maps(f->ctx, f->g1.log2n), f->ctx->T, st);
+  f->launches += 1;
   const SlotMaps maps = slot_maps(f->ctx, g2.log2n);
   const ChainConsts cc = chain_consts(f->ctx, g2.log2n, 1);
   const auto tc = f->tuned_chain.find(nb);
@@ -234,6 +242,7 @@ int fleet_secondary_kernels(dnspir_fleet* f, QSlot& s, int nb, uint8_t* reply_de
     launch_reply(f->chain_out.as<uint32_t>(), nc, g2.H, reply_dev ? reply_dev + (size_t)c0 * reply_stride : nullptr,
                  reply_stride, reply_zq ? reply_zq + (size_t)c0 * CTXT_PARTS * 2 * n : nullptr, g2.log2n, f->ctx->T,
                  st);
+    f->launches += 5;  // encoder columns, rows, lift; chains; replies
   }
   if (host_reply)
     CK(cudaMemcpyAsync(host_reply, reply_dev, (size_t)nb * dnspir_reply_bytes(), cudaMemcpyDeviceToHost, st));
@@ -281,8 +290,10 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   DeviceCtx* c = nullptr;
   CKR(get_ctx(device, &c));
   DeviceGuard dg(device);
-  CKR(ctx_consts(c, log2_n));
+  uint64_t ap_ver = 0;
+  CKR(ctx_consts(c, log2_n, &ap_ver));
   std::unique_ptr<dnspir_fleet> f(new dnspir_fleet());
+  f->ap_ver = ap_ver;
   f->device = device;
   f->ctx = c;
   f->g1 = make_group(log2_n, primary_order);
@@ -679,6 +690,16 @@ int dnspir_fleet_scan(dnspir_fleet* f, const uint32_t* qnat_dev, uint32_t nq, ui
   return fleet_drain(f);
 }
 
+int dnspir_fleet_set_wait_limit(dnspir_fleet* f, uint64_t wait_ns, int withhold_chunk) {
+  if (!f) return fail(DNSPIR_ERR_BAD_ARG, "null fleet");
+  std::lock_guard<std::mutex> lk(f->mu);
+  NOT_SERVING(f);
+  if (withhold_chunk < -1) return fail(DNSPIR_ERR_BAD_ARG, "withhold_chunk must be -1 or a chunk index");
+  f->limits.wait_ns = wait_ns;
+  f->limits.withhold = withhold_chunk;
+  return DNSPIR_OK;
+}
+
 int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int* persistent, int max) {
   int count = 0;
   const TScanShape* sh = tscan_shapes(&count);
@@ -698,6 +719,14 @@ int dnspir_fleet_set_shards(dnspir_fleet* f, uint32_t first, uint32_t count, con
   NOT_SERVING(f);
   if ((uint64_t)first + count > f->D) return fail(DNSPIR_ERR_BAD_ARG, "distinct shard index out of range");
   DeviceGuard dg(f->device);
+  {
+    // shards preprocessed under other a-parts cannot be mixed with these
+    uint64_t ver = 0;
+    CKR(ctx_consts(f->ctx, f->g1.log2n, &ver));
+    if (ver != f->ap_ver)
+      for (uint32_t d = 0; d < f->D; d++) f->ready[d] = false;
+    f->ap_ver = ver;
+  }
   const size_t per = (size_t)SIMD * f->g1.l * f->g1.n;
   const uint32_t batch = 16;
   for (uint32_t b0 = 0; b0 < count; b0 += batch) {
@@ -932,6 +961,13 @@ int dnspir_fleet_set_stream(dnspir_fleet* f, void* s) {
   std::lock_guard<std::mutex> lk(f->mu);
   NOT_SERVING(f);
   f->st = s ? (cudaStream_t)s : f->own;
+  return DNSPIR_OK;
+}
+
+int dnspir_fleet_launch_count(dnspir_fleet* f, uint64_t* count) {
+  if (!f || !count) return fail(DNSPIR_ERR_BAD_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(f->mu);
+  *count = f->launches;
   return DNSPIR_OK;
 }
 

@@ -44,6 +44,7 @@ struct dnspir_fleet {
   cudaStream_t own = nullptr, st = nullptr, sec = nullptr;
   std::vector<uint32_t*> slabs;
   std::vector<bool> ready;
+  uint64_t ap_ver = 0;  // a-parts version every ready shard was preprocessed under
   dnspir::DBuf slabs_dev, distinct_dev, a_zq, a_ms;
   dnspir::EncodeWs ws;
   dnspir::QSlot slot[2];
@@ -54,6 +55,7 @@ struct dnspir_fleet {
   int engine = DNSPIR_ENGINE_CUDA_CORES;
   bool serving = false;                       // attached to a running server
   dnspir::DBuf qb, err_word, tmp_lane;        // tensor engine: query operand, wait-error word, preprocessing scratch
+  dnspir::TScanLimits limits;                 // tensor engine: wait limit (and the timeout-test hook)
   std::map<int, int> tuned;                   // tensor engine: group size -> tile shape index
   std::map<int, int> tuned_cc;                // CUDA-core engine: group size -> queries per block
   std::map<int, int> tuned_chain;             // group size -> 1: two-block-cluster chains at every chunk size
@@ -62,6 +64,7 @@ struct dnspir_fleet {
                                               // reaches its last chunk
   std::vector<cudaEvent_t> tev;               // 6 timing events per group of the last call
   std::vector<int> q_group;                   // per query of the last call: its group, or -1
+  uint64_t launches = 0;                      // kernels launched by the answer pipeline so far
   std::mutex mu;
   ~dnspir_fleet();
 };

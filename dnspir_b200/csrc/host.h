@@ -5,6 +5,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "dnspir.h"
 #include "kernels.cuh"
@@ -34,6 +35,8 @@ struct DeviceCtx {
   uint32_t* tables = nullptr;
   NttTables T;
   uint32_t* consts[LOG2_N_MAX + 1] = {};  // a-parts in NTT form: [6][2][N], bit-reversed positions
+  uint64_t consts_ver[LOG2_N_MAX + 1] = {};  // a-parts version they were built from
+  std::vector<uint32_t*> retired;            // a-part buffers replaced by dnspir_set_a_parts
   uint32_t* galb[LOG2_N_MAX + 1] = {};
   uint32_t* gtab[LOG2_N_MAX + 1] = {};  // scan slot order: position -> odd residue
   uint32_t* uof[LOG2_N_MAX + 1] = {};   // natural slot -> position
@@ -107,7 +110,14 @@ struct DeviceGuard {
 };
 
 int get_ctx(int device, DeviceCtx** out);
-int ctx_consts(DeviceCtx* c, int log2n);
+// Per-dimension constants of a device; also brings the a-parts in NTT form up
+// to the a-parts now in effect, whose version goes to *version.
+int ctx_consts(DeviceCtx* c, int log2n, uint64_t* version = nullptr);
+// The six a-parts in effect for dimension 2^log2n (6 x N coefficients in
+// [0, q): gk0, gk1, FirstSet query, its conjugate, SecondSet query, its
+// conjugate) and their version.
+void a_parts_host(int log2n, uint64_t* out, uint64_t* version);
+uint64_t a_parts_version(int log2n);
 SlotMaps slot_maps(DeviceCtx* c, int log2n);
 ChainConsts chain_consts(DeviceCtx* c, int log2n, int used_seeds);
 int check_group(uint32_t log2n, uint32_t l);

@@ -102,16 +102,26 @@ void tensor_dims(const Group& g, uint32_t* mt_total, uint32_t* kc_total);
 void launch_retile(const uint32_t* lane_slab, uint8_t* tensor_slab, const Group& g, cudaStream_t st);
 const TScanShape* tscan_shapes(int* count);
 size_t tscan_query_bytes(const Group& g, int nb_pad);
+// Limits of the tensor scan's pipeline waits: wait_ns (0: the default, 2 s)
+// and, for tests of the timeout path, a chunk that CTA 0's producer never
+// copies (withhold >= 0), so that its MMA thread's wait runs out.
+struct TScanLimits {
+  uint64_t wait_ns = 0;
+  int withhold = -1;
+};
 // nb queries (decoded, qnat) padded to nb_pad (a multiple of shape.nq / 4);
 // qb: tscan_query_bytes of workspace; out as launch_scan_batch; err: one
 // device word set to 1 when a bounded wait gave up.  Returns -1 for a shape
 // that does not fit.
 int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int nb, int nb_pad,
                  uint8_t* qb, uint32_t* out, uint32_t* err, const Group& g, const SlotMaps& maps,
-                 const TScanShape& shape, cudaStream_t st);
+                 const TScanShape& shape, cudaStream_t st, const TScanLimits& lim = TScanLimits());
 // Per-lane queries (perform_pir_split): qlane [(lane*4 + v)*2 + p][N] natural order;
 // part: [chunk][p][u][lane], chunks = H * R.
 int scan_chunks(const Group& g, int nshards);
+// Loads the kernels of launch_scan_lanes and launch_epilogue_zq on the current
+// device (0, or -1 on a CUDA error).
+int preload_pir_split_kernels();
 void launch_scan_lanes(const uint32_t* slab, const uint32_t* qlane, uint32_t* part, const Group& g, int R,
                        const SlotMaps& maps, cudaStream_t st);
 // Primary epilogue for nq queries: scan output -> b (iNTT, CRT), mod-switch,

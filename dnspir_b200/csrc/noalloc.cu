@@ -9,14 +9,19 @@
 // fixed-size region of device memory that is part of this library's module:
 // the caller passes device inputs and outputs, the call allocates nothing.
 //
-// The region is a file-scope __device__ array, so every GPU that loads the
-// library holds it (NOALLOC_SCRATCH_BYTES) until the process exits.  Host code
-// cannot use the array's name as a device address; the first call on each
-// device looks its address up with cudaGetSymbolAddress while that device is
-// current (make that first call before any stream capture) and keeps it.
+// The region is a file-scope __device__ array (NOALLOC_SCRATCH_BYTES).  The
+// CUDA runtime loads this library's device code lazily, so the region is
+// reserved on a device when dnspir_db_create first runs there: that call looks
+// its address up with cudaGetSymbolAddress while the device is current (before
+// the shard's slab takes the memory) and keeps it; from then on the device
+// holds the region until the process exits.  Host code cannot use the array's
+// name as a device address; only the looked-up address is passed to kernels.
 // All calls on a device share the region: two calls whose work overlaps on
 // the GPU (different streams, no ordering between them) race and corrupt each
 // other's answers; order them on one stream or synchronize between them.
+// The call holds the shard's lock while it queues its work and records an
+// event on the caller's stream; dnspir_db_set_db and dnspir_db_destroy wait
+// for that event before they touch the slab.
 // Nothing in the region has to start at zero: each call writes every byte of
 // it that it later reads.
 #include <cstdio>
@@ -37,8 +42,11 @@ constexpr int NOALLOC_MAX_CHUNKS = 16;
 constexpr size_t NOALLOC_PART_BYTES = (size_t)2 * NOALLOC_MAX_CHUNKS * 2 * N_MAX * SIMD * 4;
 constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_ZQ_BYTES + NOALLOC_NTT_BYTES + NOALLOC_PART_BYTES;
 
-// What the entry point needs from a shard (defined in api.cu).
-int db_view(const dnspir_db* db, DbView* out);
+// What the entry point needs from a shard (defined in api.cu): begin locks
+// the shard and fills the view (unlocked again on failure); end records the
+// shard's completion event on the stream and unlocks.
+int db_noalloc_begin(dnspir_db* db, DbView* out);
+int db_noalloc_end(dnspir_db* db, cudaStream_t st);
 void set_last_error(const std::string& msg);
 
 }  // namespace dnspir
@@ -72,6 +80,25 @@ static int noalloc_scratch(int device, unsigned char** out) {
   return DNSPIR_OK;
 }
 
+namespace dnspir {
+// Reserves the region on `device` (which must be current): loads it, looks
+// its address up and loads the kernels the entry point launches, so that its
+// calls need no device memory of their own.  Called by dnspir_db_create.
+int noalloc_reserve(int device) {
+  unsigned char* p = nullptr;
+  const int rc = noalloc_scratch(device, &p);
+  if (rc != DNSPIR_OK) return rc;
+  if (preload_pir_split_kernels() != 0) {
+    set_last_error("cannot load the single-shard scan kernels");
+    return DNSPIR_ERR_CUDA;
+  }
+  return DNSPIR_OK;
+}
+}  // namespace dnspir
+
+static int noalloc_queue(const DbView& v, const uint64_t* qry_b, const uint64_t* qry_conj_b, const uint64_t* gk_b,
+                         uint64_t* out_b, cudaStream_t st);
+
 extern "C" int dnspir_db_perform_pir_split_noalloc(dnspir_db* db, const uint64_t* qry_b, const uint64_t* qry_conj_b,
                                                    const uint64_t* gk_b, uint64_t* out_b, void* cuda_stream) {
   if (!db || !qry_b || !gk_b || !out_b) {
@@ -79,12 +106,17 @@ extern "C" int dnspir_db_perform_pir_split_noalloc(dnspir_db* db, const uint64_t
     return DNSPIR_ERR_BAD_ARG;
   }
   DbView v;
-  int rc = db_view(db, &v);
+  int rc = db_noalloc_begin(db, &v);  // locks the shard
   if (rc != DNSPIR_OK) return rc;
-  if (!v.ready) {
-    set_last_error("database not preprocessed");
-    return DNSPIR_ERR_NOT_READY;
-  }
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  rc = noalloc_queue(v, qry_b, qry_conj_b, gk_b, out_b, st);
+  const int rc_end = db_noalloc_end(db, st);  // unlocks
+  return rc != DNSPIR_OK ? rc : rc_end;
+}
+
+static int noalloc_queue(const DbView& v, const uint64_t* qry_b, const uint64_t* qry_conj_b, const uint64_t* gk_b,
+                         uint64_t* out_b, cudaStream_t st) {
+  int rc = DNSPIR_OK;
   const Group& g = v.g;
   if ((g.H == 2) != (qry_conj_b != nullptr)) {
     set_last_error("conjugate query must be given exactly when the group requires it");
@@ -104,18 +136,23 @@ extern "C" int dnspir_db_perform_pir_split_noalloc(dnspir_db* db, const uint64_t
     return DNSPIR_ERR_BAD_SIZE;
   }
   int prev = -1;
-  cudaGetDevice(&prev);
-  if (prev != v.device) cudaSetDevice(v.device);
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e == cudaSuccess && prev != v.device) e = cudaSetDevice(v.device);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("no-allocation perform_pir_split: cannot make the shard's device current: ") +
+                   cudaGetErrorString(e));
+    return DNSPIR_ERR_CUDA;
+  }
   unsigned char* scratch = nullptr;
   rc = noalloc_scratch(v.device, &scratch);
   if (rc == DNSPIR_OK) {
-    cudaStream_t st = (cudaStream_t)cuda_stream;
     uint64_t* zq = (uint64_t*)scratch;
     uint32_t* ntt = (uint32_t*)(scratch + NOALLOC_ZQ_BYTES);
     uint32_t* part = (uint32_t*)(scratch + NOALLOC_ZQ_BYTES + NOALLOC_NTT_BYTES);
     // gather: lane k's polynomials land at slots 4k + {0: qry, 1: qry_conj, 2: gk0, 3: gk1}
     const size_t row = n * 8, pitch = 4 * row;
-    cudaError_t e = cudaMemcpy2DAsync(zq, pitch, qry_b, row, row, SIMD, cudaMemcpyDeviceToDevice, st);
+    e = cudaMemcpy2DAsync(zq, pitch, qry_b, row, row, SIMD, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess)
       e = qry_conj_b ? cudaMemcpy2DAsync((char*)zq + row, pitch, qry_conj_b, row, row, SIMD, cudaMemcpyDeviceToDevice, st)
                      : cudaMemset2DAsync((char*)zq + row, pitch, 0, row, SIMD, st);

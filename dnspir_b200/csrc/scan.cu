@@ -392,6 +392,18 @@ void launch_primary_epilogue(const uint32_t* fin, int nq, int nshards, const uin
                                                    maps.uof, T, host_crt_const());
 }
 
+int preload_pir_split_kernels() {
+  // the runtime loads kernels lazily, at their first launch; this loads the
+  // single-shard scan kernels now (cudaFuncGetAttributes forces the load)
+  cudaFuncAttributes a;
+  if (cudaFuncGetAttributes(&a, (const void*)scan_lanes_kernel) != cudaSuccess ||
+      cudaFuncGetAttributes(&a, (const void*)epilogue_zq_kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return 0;
+}
+
 void launch_epilogue_zq(const uint32_t* part, int chunks, uint64_t* out, const Group& g, const SlotMaps& maps,
                         const NttTables& T, cudaStream_t st) {
   const size_t smem = (size_t)4 * g.n * 4;

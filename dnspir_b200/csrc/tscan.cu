@@ -65,12 +65,12 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for the phase of `parity` to complete; false after WAIT_NS.
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Wait for the phase of `parity` to complete; false after limit_ns.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = gtimer();
   while (!mbar_try(bar, parity))
-    if (gtimer() - t0 > WAIT_NS) return false;
+    if (gtimer() - t0 > limit_ns) return false;
   return true;
 }
 
@@ -130,6 +130,8 @@ struct TScanArgs {
   uint32_t* out;      // [b][s][p][u][lane]
   uint32_t* err;      // set to 1 when a wait gives up
   uint32_t half, mt_total, kc_total, groups, stages;
+  uint64_t wait_ns;   // limit of every pipeline wait
+  uint32_t withhold;  // test hook: CTA 0's producer stops before this chunk (~0u: never)
 };
 
 template <int NQ, int MTPC>
@@ -192,7 +194,8 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
     uint32_t issued = 0;
     for (uint32_t kc = 0; kc < KC; kc++) {
       const uint32_t st = kc % S_, n = kc / S_;
-      if (n > 0 && !mbar_wait(&empty[st], (n - 1) & 1)) {
+      if (blockIdx.x == 0 && kc == a.withhold) break;  // test hook: a chunk that never arrives
+      if (n > 0 && !mbar_wait(&empty[st], (n - 1) & 1, a.wait_ns)) {
         atomicOr(a.err, 1u);
         break;
       }
@@ -210,7 +213,7 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
     uint32_t consumed = 0;
     for (uint32_t kc = 0; kc < KC; kc++) {
       const uint32_t st = kc % S_, n = kc / S_;
-      if (!mbar_wait(&full[st], n & 1)) {
+      if (!mbar_wait(&full[st], n & 1, a.wait_ns)) {
         atomicOr(a.err, 1u);
         break;
       }
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
   __syncwarp();
 
   // epilogue: warp w holds TMEM lanes 32w..32w+31 = rows of slot e = 4 mt + w
-  const bool acc_ok = mbar_wait(accb, 0);
+  const bool acc_ok = mbar_wait(accb, 0, a.wait_ns);
   tc_fence_after();
   if (acc_ok) {
     const uint32_t pr = prime_of(p);
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
   if (threadIdx.x == 0) {
     // copies issued but never consumed (only after a wait gave up) must land
     // before the shared memory is released
-    for (uint32_t kc = *consumed_s; kc < *issued_s; kc++) mbar_wait(&full[kc % S_], (kc / S_) & 1);
+    for (uint32_t kc = *consumed_s; kc < *issued_s; kc++) mbar_wait(&full[kc % S_], (kc / S_) & 1, a.wait_ns);
   }
   __syncthreads();
   if (warp == 2) {
@@ -370,7 +373,8 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
   if (warp == 0) {
     if (lane == 0) {
       uint32_t g = 0;
-      for (uint32_t item = blockIdx.x; item < items && !*abort_s; item += gridDim.x) {
+      bool withheld = false;
+      for (uint32_t item = blockIdx.x; item < items && !*abort_s && !withheld; item += gridDim.x) {
         uint32_t grp, mt0, sgn;
         int p, s;
         tile_of(item, grp, mt0, sgn, p, s);
@@ -379,7 +383,11 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
         const uint8_t* bbase = a.qb + ps * KC * a.nq_rows * 128 + (size_t)grp * NQ * 128;
         for (uint32_t kc = 0; kc < KC; kc++, g++) {
           const uint32_t st = g % S_, n = g / S_;
-          if (n > 0 && !mbar_wait(&empty[st], (n - 1) & 1)) {
+          if (blockIdx.x == 0 && g == a.withhold) {  // test hook: a chunk that never arrives
+            withheld = true;
+            break;
+          }
+          if (n > 0 && !mbar_wait(&empty[st], (n - 1) & 1, a.wait_ns)) {
             *abort_s = 1;
             atomicOr(a.err, 1u);
             break;
@@ -400,7 +408,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
       uint32_t g = 0, j = 0;
       for (uint32_t item = blockIdx.x; item < items && !*abort_s; item += gridDim.x, j++) {
         const uint32_t buf = j & 1, use = j >> 1;
-        if (use > 0 && !mbar_wait(&acce[buf], (use - 1) & 1)) {
+        if (use > 0 && !mbar_wait(&acce[buf], (use - 1) & 1, a.wait_ns)) {
           *abort_s = 1;
           atomicOr(a.err, 1u);
           break;
@@ -409,7 +417,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
         bool ok = true;
         for (uint32_t kc = 0; kc < KC; kc++, g++) {
           const uint32_t st = g % S_, n = g / S_;
-          if (!mbar_wait(&full[st], n & 1)) {
+          if (!mbar_wait(&full[st], n & 1, a.wait_ns)) {
             *abort_s = 1;
             atomicOr(a.err, 1u);
             ok = false;
@@ -438,7 +446,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
     uint32_t j = 0;
     for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, j++) {
       const uint32_t buf = j & 1, use = j >> 1;
-      if (!mbar_wait(&accf[buf], use & 1)) {
+      if (!mbar_wait(&accf[buf], use & 1, a.wait_ns)) {
         if (lane == 0) {
           *abort_s = 1;
           atomicOr(a.err, 1u);
@@ -487,17 +495,330 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
     }
   }
   __syncthreads();
-  if (threadIdx.x == 32) mbar_wait(done, 0);  // every MMA issued by the CTA has completed
+  if (threadIdx.x == 32) mbar_wait(done, 0, a.wait_ns);  // every MMA issued by the CTA has completed
   if (threadIdx.x == 0) {
     // copies issued but never consumed (only after a wait gave up) must land
     // before the shared memory is released
-    for (uint32_t g = *consumed_s; g < *issued_s; g++) mbar_wait(&full[g % S_], (g / S_) & 1);
+    for (uint32_t g = *consumed_s; g < *issued_s; g++) mbar_wait(&full[g % S_], (g / S_) & 1, a.wait_ns);
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+  }
+}
+
+// ---- CTA-pair variant: tcgen05.mma.cta_group::2, persistent, warp-specialised.
+// A cluster of two CTAs works on one item at a time: 2 x MTPC m-tiles of one
+// (shard, factor, sign) against one query group.  CTA r keeps m-tiles
+// mt0 + r MTPC + t (t < MTPC) in its shared memory and half of the group's
+// query-operand rows (grp NQ + r NQ/2 ..); the leader (rank 0) issues M = 256
+// MMAs that read both CTAs' operands, and each CTA's TMEM receives its own 128
+// rows x NQ columns per m-tile.  Compared with the one-CTA kernels every SM
+// stages only half of the query operand per chunk, so a ring of the same size
+// holds more chunks.  Roles, in each CTA: warp 0 lane 0 streams the CTA's
+// chunks into its ring (bulk copies, local full barrier); warp 1 lane 0 is the
+// MMA issuer in the leader and, in the follower, the relay that forwards each
+// completed stage to the leader's pfull barrier; warps 2-5 read the TMEM
+// accumulators and write the residues.  The leader's commits arrive on both
+// CTAs' barriers (multicast commit); the epilogue warps of both CTAs release
+// an accumulator on the leader's acce barrier.  Accumulators are
+// double-buffered when 2 MTPC NQ <= 512 TMEM columns.  Every wait is bounded
+// and also gives up once either CTA has raised the pair's abort flag; a CTA
+// then waits (bounded) for its MMAs and copies in flight before it frees TMEM.
+constexpr int TSCAN2_NT = 192;
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_idx() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same shared-memory offset in CTA `rank`
+__device__ __forceinline__ uint32_t peer_addr(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(sa(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_peer(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, "
+      "p;\n}\n"
+      : "=r"(ok)
+      : "r"(sa(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// The phase of `parity` completed (true), or limit_ns passed or the pair's
+// abort flag was raised (false).
+__device__ bool mbar_wait_pair(uint64_t* bar, uint32_t parity, uint64_t limit_ns, volatile uint32_t* abort_flag,
+                               bool cluster_scope) {
+  auto done = [&] { return cluster_scope ? mbar_try_cluster(bar, parity) : mbar_try(bar, parity); };
+  if (done()) return true;
+  const uint64_t t0 = gtimer();
+  for (;;) {
+    if (done()) return true;
+    if (*abort_flag) return false;
+    if (gtimer() - t0 > limit_ns) return false;
+  }
+}
+// raise the abort flag of both CTAs of the pair and the error word
+__device__ __forceinline__ void pair_abort(volatile uint32_t* abort_flag, uint32_t* err) {
+  *abort_flag = 1;
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_addr((const void*)abort_flag, cluster_rank() ^ 1)),
+               "r"(1u)
+               : "memory");
+  atomicOr(err, 1u);
+}
+__device__ __forceinline__ void mma2_u8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// arrive on the barrier at this offset in both CTAs once the leader's MMAs issued so far complete
+__device__ __forceinline__ void mma2_commit_both(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          sa(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+
+template <int NQ, int MTPC>
+__global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
+  constexpr uint32_t A_BYTES = MTPC * TBLK;
+  constexpr uint32_t V_BYTES = NQ / 2 * 128;  // this CTA's half of the group's query rows
+  constexpr uint32_t STAGE = A_BYTES + V_BYTES;
+  constexpr uint32_t ACC = MTPC * NQ;  // TMEM columns of one accumulator
+  constexpr uint32_t BUFS = 2 * ACC <= 512 ? 2 : 1;
+  constexpr uint32_t COLS = BUFS * ACC < 32 ? 32 : BUFS * ACC;
+  static_assert(NQ >= 32 && NQ <= 256 && NQ % 32 == 0, "pair MMA: N in 32..256, a multiple of 32");
+  static_assert(STAGE % 1024 == 0 && ACC <= 512 && (COLS & (COLS - 1)) == 0, "tile shape");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t S_ = a.stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + S_ * STAGE);
+  uint64_t* empty = full + S_;
+  uint64_t* pfull = empty + S_;  // leader: the follower's stage landed
+  uint64_t* accf = pfull + S_;   // [2] accumulator ready (multicast commit)
+  uint64_t* acce = accf + 2;     // [2] accumulator drained (leader: 4 local + 4 remote warps)
+  uint64_t* done = acce + 2;     // every MMA of the pair complete (multicast commit)
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile uint32_t* issued_s = tslot + 1;
+  volatile uint32_t* abort_s = tslot + 2;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const uint32_t rank = cluster_rank();
+  const uint32_t mtc = a.mt_total / (2 * MTPC);  // m-tile groups of a pair
+  const uint32_t items = (uint32_t)a.nshards * 4 * mtc * a.groups;
+  const uint32_t KC = a.kc_total;
+  const uint32_t cid = cluster_idx(), ncl = cluster_count();
+
+  if (threadIdx.x == 0) {
+    for (uint32_t i = 0; i < S_; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+      mbar_init(&pfull[i], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 8);
+    }
+    mbar_init(done, 1);
+    *issued_s = 0;
+    *abort_s = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(tslot)), "r"(COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // both CTAs' barriers exist before any remote arrive or MMA
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  auto tile_of = [&](uint32_t item, uint32_t& grp, uint32_t& mt0, uint32_t& sgn, int& p, int& s) {
+    grp = item % a.groups;
+    item /= a.groups;
+    mt0 = (item % mtc) * 2 * MTPC;
+    item /= mtc;
+    sgn = item & 1;
+    p = (item >> 1) & 1;
+    s = item >> 2;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t g = 0;
+      bool stop = false;
+      for (uint32_t item = cid; item < items && !stop; item += ncl) {
+        uint32_t grp, mt0, sgn;
+        int p, s;
+        tile_of(item, grp, mt0, sgn, p, s);
+        const size_t ps = (size_t)p * 2 + sgn;
+        const uint8_t* abase = a.slabs[s] + (ps * a.mt_total + mt0 + rank * MTPC) * KC * TBLK;
+        const uint8_t* bbase = a.qb + ps * KC * a.nq_rows * 128 + ((size_t)grp * NQ + rank * (NQ / 2)) * 128;
+        for (uint32_t kc = 0; kc < KC; kc++, g++) {
+          const uint32_t st = g % S_, n = g / S_;
+          if (blockIdx.x == 0 && g == a.withhold) {  // test hook: a chunk that never arrives
+            stop = true;
+            break;
+          }
+          if (n > 0 && !mbar_wait_pair(&empty[st], (n - 1) & 1, a.wait_ns, abort_s, false)) {
+            if (!*abort_s) pair_abort(abort_s, a.err);
+            stop = true;
+            break;
+          }
+          uint8_t* dst = sm + st * STAGE;
+          mbar_expect_tx(&full[st], STAGE);
+#pragma unroll
+          for (int t = 0; t < MTPC; t++)
+            bulk_g2s(dst + t * TBLK, abase + ((size_t)t * KC + kc) * TBLK, TBLK, &full[st]);
+          bulk_g2s(dst + A_BYTES, bbase + (size_t)kc * a.nq_rows * 128, V_BYTES, &full[st]);
+          *issued_s = g + 1;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank != 0) {
+      // relay: each stage of this CTA that lands is announced to the leader
+      const uint32_t total = ((items > cid ? (items - cid + ncl - 1) / ncl : 0)) * KC;
+      for (uint32_t g = 0; g < total; g++) {
+        const uint32_t st = g % S_, n = g / S_;
+        if (!mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, false)) {
+          if (!*abort_s) pair_abort(abort_s, a.err);
+          break;
+        }
+        mbar_arrive_peer(peer_addr(&pfull[st], 0));
+      }
+    } else if (lane == 0) {
+      constexpr uint32_t idesc = idesc_u8(256, NQ);
+      uint32_t g = 0, j = 0;
+      bool stop = false;
+      for (uint32_t item = cid; item < items && !stop; item += ncl, j++) {
+        const uint32_t buf = j % BUFS, use = j / BUFS;
+        if (use > 0 && !mbar_wait_pair(&acce[buf], (use - 1) & 1, a.wait_ns, abort_s, true)) {
+          if (!*abort_s) pair_abort(abort_s, a.err);
+          break;
+        }
+        tc_fence_after();
+        for (uint32_t kc = 0; kc < KC; kc++, g++) {
+          const uint32_t st = g % S_, n = g / S_;
+          if (!mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, false) ||
+              !mbar_wait_pair(&pfull[st], n & 1, a.wait_ns, abort_s, true)) {
+            if (!*abort_s) pair_abort(abort_s, a.err);
+            stop = true;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t s0 = sa(sm + st * STAGE);
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int t = 0; t < MTPC; t++)
+              mma2_u8(tmem + buf * ACC + t * NQ, sw128_desc(s0 + t * TBLK + 32 * k),
+                      sw128_desc(s0 + A_BYTES + 32 * k), idesc, (kc | k) != 0);
+          mma2_commit_both(&empty[st]);
+        }
+        if (stop) break;
+        mma2_commit_both(&accf[buf]);
+      }
+      mma2_commit_both(done);
+    }
+  } else {
+    const int q = warp & 3;  // TMEM lane quarter = slot e mod 4 of the m-tile
+    const int k = lane & 3, l8 = lane >> 2;
+    const uint32_t N = 2 * a.half;
+    const uint32_t acce_leader = peer_addr(&acce[0], 0);
+    uint32_t j = 0;
+    for (uint32_t item = cid; item < items; item += ncl, j++) {
+      const uint32_t buf = j % BUFS, use = j / BUFS;
+      if (!mbar_wait_pair(&accf[buf], use & 1, a.wait_ns, abort_s, false)) {
+        if (lane == 0 && !*abort_s) pair_abort(abort_s, a.err);
+        break;
+      }
+      tc_fence_after();
+      uint32_t grp, mt0, sgn;
+      int p, s;
+      tile_of(item, grp, mt0, sgn, p, s);
+      const uint32_t pr = prime_of(p);
+      const uint64_t mu = barrett_mu(pr);
+      const uint64_t c32 = reduce64(1ull << 32, pr, mu);
+      const uint64_t c40 = reduce64(c32 << 8, pr, mu);
+      const uint64_t c48 = reduce64(c40 << 8, pr, mu);
+      const uint32_t w3 = (uint32_t)reduce64(1ull << 24, pr, mu);
+      const uint32_t c0 = k == 0 ? 1u : k == 1 ? 256u : k == 2 ? 65536u : w3;
+      const uint32_t c1 = k == 0 ? 256u : k == 1 ? 65536u : k == 2 ? w3 : (uint32_t)c32;
+      const uint32_t c2 = k == 0 ? 65536u : k == 1 ? w3 : k == 2 ? (uint32_t)c32 : (uint32_t)c40;
+      const uint32_t c3 = k == 0 ? w3 : k == 1 ? (uint32_t)c32 : k == 2 ? (uint32_t)c40 : (uint32_t)c48;
+      for (int t = 0; t < MTPC; t++) {
+        const uint32_t u = sgn * a.half + 4 * (mt0 + rank * MTPC + t) + q;
+#pragma unroll 1
+        for (int q4 = 0; q4 < NQ / 16; q4++) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ + 16 * q4, v);
+          uint64_t tot[4];
+#pragma unroll
+          for (int qq = 0; qq < 4; qq++) {
+            uint64_t x = (uint64_t)v[4 * qq] * c0 + (uint64_t)v[4 * qq + 1] * c1 + (uint64_t)v[4 * qq + 2] * c2 +
+                         (uint64_t)v[4 * qq + 3] * c3;
+            x += __shfl_xor_sync(0xffffffffu, x, 1);
+            x += __shfl_xor_sync(0xffffffffu, x, 2);
+            tot[qq] = x;
+          }
+          const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
+          const uint32_t bq = grp * (NQ / 4) + 4 * q4 + k;
+          if (bq < a.nvalid)
+            a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if (rank == 0)
+          mbar_arrive(&acce[buf]);
+        else
+          mbar_arrive_peer(acce_leader + buf * 8);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 32) mbar_wait(done, 0, a.wait_ns);  // every MMA of the pair has completed
+  if (threadIdx.x == 0 && *abort_s) {
+    // copies issued but perhaps never consumed must land before the shared
+    // memory is released (only after a wait gave up)
+    const uint32_t iss = *issued_s;
+    for (uint32_t g = iss > S_ ? iss - S_ : 0; g < iss; g++) mbar_wait(&full[g % S_], (g / S_) & 1, a.wait_ns);
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // neither CTA leaves while the peer may still touch its barriers
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
   }
 }
 
@@ -616,6 +937,41 @@ int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
   return 0;
 }
 
+template <int NQ, int MTPC>
+int launch_t2(const TScanArgs& a0, int stages, cudaStream_t st) {
+  TScanArgs a = a0;
+  a.stages = (uint32_t)stages;
+  constexpr uint32_t STAGE = MTPC * TBLK + NQ / 2 * 128;
+  const size_t smem = 1024 + (size_t)stages * STAGE + (3 * stages + 5) * 8 + 16;
+  if (smem > 227 * 1024 || a.mt_total % (2 * MTPC)) return -1;
+  set_smem(tscan2_kernel<NQ, MTPC>, smem);
+  const size_t items = (size_t)a.nshards * 4 * (a.mt_total / (2 * MTPC)) * a.groups;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(TSCAN2_NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(2);
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, tscan2_kernel<NQ, MTPC>, &cfg) != cudaSuccess || clusters < 1) {
+    cudaGetLastError();
+    return -1;
+  }
+  // one CTA per SM: TMEM columns of a resident CTA never exceed the SM's 512
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  clusters = std::min(clusters, sms / 2);
+  cfg.gridDim = dim3((unsigned)(2 * std::min<size_t>(items, (size_t)clusters)));
+  return cudaLaunchKernelEx(&cfg, tscan2_kernel<NQ, MTPC>, a) == cudaSuccess ? 0 : -1;
+}
+
 }  // namespace
 
 int tensor_layout_supported(const Group& g) { return g.log2n >= 8 && g.L == g.n / 2 && g.H >= 1; }
@@ -644,6 +1000,9 @@ const TScanShape* tscan_shapes(int* count) {
       {128, 1, 3, 0}, {128, 2, 2, 0}, {128, 2, 3, 0}, {256, 1, 2, 0}, {256, 1, 3, 0}, {256, 1, 4, 0},
       {256, 2, 2, 0}, {256, 2, 3, 0}, {512, 1, 2, 0}, {16, 1, 6, 1},  {64, 1, 5, 1},  {64, 2, 4, 1},
       {128, 1, 4, 1}, {128, 2, 3, 1}, {256, 1, 3, 1}, {256, 1, 4, 1},
+      // CTA pairs (tcgen05.mma.cta_group::2): rows are the pair's query
+      // operand rows (each CTA stages half of them)
+      {64, 1, 8, 2},  {128, 1, 6, 2}, {128, 2, 4, 2}, {256, 1, 6, 2}, {256, 2, 4, 2},
   };
   *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
   return shapes;
@@ -657,7 +1016,7 @@ size_t tscan_query_bytes(const Group& g, int nb_pad) {
 
 int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int nb, int nb_pad,
                  uint8_t* qb, uint32_t* out, uint32_t* err, const Group& g, const SlotMaps& maps,
-                 const TScanShape& shape, cudaStream_t st) {
+                 const TScanShape& shape, cudaStream_t st, const TScanLimits& lim) {
   uint32_t mt, kc;
   tensor_dims(g, &mt, &kc);
   const int qpc = shape.nq / 4;
@@ -679,7 +1038,19 @@ int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, s
   a.kc_total = kc;
   a.groups = nb_pad / qpc;
   a.stages = 0;
+  a.wait_ns = lim.wait_ns ? lim.wait_ns : WAIT_NS;
+  a.withhold = lim.withhold < 0 ? ~0u : (uint32_t)lim.withhold;
   const int stg = shape.stages;
+  if (shape.persistent == 2) {
+    switch (shape.nq * 10 + shape.mtpc) {
+      case 641: return launch_t2<64, 1>(a, stg, st);
+      case 1281: return launch_t2<128, 1>(a, stg, st);
+      case 1282: return launch_t2<128, 2>(a, stg, st);
+      case 2561: return launch_t2<256, 1>(a, stg, st);
+      case 2562: return launch_t2<256, 2>(a, stg, st);
+      default: return -1;
+    }
+  }
   if (shape.persistent) {
     switch (shape.nq * 10 + shape.mtpc) {
       case 161: return launch_tp<16, 1>(a, stg, st);

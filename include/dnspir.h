@@ -55,8 +55,28 @@ uint64_t dnspir_query_bytes(uint32_t primary_order, uint32_t secondary_order);
 uint64_t dnspir_reply_bytes(void);
 
 /* expand (bfv.rs:46-49) of SEEDS[which] (base_pir.rs:64-71) for ring dimension
- * 2^log2_n: out = N coefficients in [0, q).  Host only; needs no device. */
+ * 2^log2_n: out = N coefficients in [0, q).  Host only; needs no device.
+ * Coefficient i is drawn in order i = 0..N-1 from the StdRng (ChaCha12) stream
+ * keyed by the seed: the low ceil(log2 q) = 51 bits of one next_u64, drawn
+ * again while >= q (the uniform-below-bound rule that feanor-math's
+ * random_element applies per coefficient, as this library restates it). */
 int dnspir_expand_seed(uint32_t log2_n, int which, uint64_t* out);
+/* The six a-parts of ring dimension 2^log2_n, process-wide: the fixed `a`
+ * polynomials every query ciphertext and Galois key shares (bfv.rs:46-49 via
+ * UsedSeeds, base_pir.rs:104-107, 193-205; computed once in
+ * PIRDatabase::create / preprocess, base_pir.rs:782-789).  coeffs = 6 x N
+ * values in [0, q) in the order gk0, gk1, FirstSet query, FirstSet conjugate
+ * query, SecondSet query, SecondSet conjugate query; NULL restores the seed
+ * expansion (dnspir_expand_seed of SEEDS[0..5]).  This is the hook for a-parts
+ * produced by the reference itself: with them installed, reply bytes are
+ * comparable with the reference's.  Databases and fleets preprocessed under
+ * other a-parts answer DNSPIR_ERR_NOT_READY until their set_db / set_shards
+ * runs again; do not call it while a call on a database of that dimension is
+ * running.  The client calls (dnspir_client_*) use the same a-parts. */
+int dnspir_set_a_parts(uint32_t log2_n, const uint64_t* coeffs);
+/* The six a-parts in effect for ring dimension 2^log2_n (6 x N coefficients,
+ * order as dnspir_set_a_parts). */
+int dnspir_get_a_parts(uint32_t log2_n, uint64_t* out);
 
 /* ---- one preprocessed shard: PIRDatabase (base_pir.rs:229-255) --------- */
 
@@ -83,10 +103,12 @@ int dnspir_db_destroy(dnspir_db* db);
  * arrays are DEVICE pointers with the layouts of dnspir_db_perform_pir_split;
  * coefficients must already be below q (not checked).  Work is queued on
  * cuda_stream (NULL = the default stream) and the call returns without waiting.
- * Intermediates live in a static 5 MiB region of device memory that every GPU
- * loading the library holds until exit; nothing is allocated.  The first call
- * on a device looks that region up (make it before any stream capture).  Calls
- * on one device share the region: calls whose work overlaps on the GPU race. */
+ * Intermediates live in a static 5 MiB region of device memory; nothing is
+ * allocated.  The region (and the kernels this call launches) is loaded on a
+ * device by the first dnspir_db_create there, which also looks its address up,
+ * and the device holds it until exit.  Calls on one device share the region:
+ * calls whose work overlaps on the GPU race.  dnspir_db_set_db and
+ * dnspir_db_destroy wait for the work of earlier calls on their shard. */
 int dnspir_db_perform_pir_split_noalloc(dnspir_db* db, const uint64_t* qry_b, const uint64_t* qry_conj_b,
                                         const uint64_t* gk_b, uint64_t* out_b, void* cuda_stream);
 
@@ -170,6 +192,15 @@ int dnspir_fleet_get_schedule(dnspir_fleet* fleet, uint32_t batch, int* schedule
  * groups of `batch` queries, overriding the table or a previous tune; -1
  * returns to the default.  No counterpart in the reference. */
 int dnspir_fleet_set_tile(dnspir_fleet* fleet, uint32_t batch, int shape_index);
+/* Tensor engine: limit of every wait in the scan's copy/MMA/epilogue pipeline
+ * (wait_ns; 0 restores the default of 2 s).  A wait that runs out makes the
+ * scan's blocks stop, wait (bounded) for their copies in flight, free their
+ * tensor memory and return; the call then fails with DNSPIR_ERR_TIMEOUT and
+ * the device stays usable.  withhold_chunk >= 0 is a test hook for that path:
+ * the first block's producer stops before copying that chunk, so the block's
+ * MMA thread waits for a copy that never comes (-1: off).  No counterpart in
+ * the reference. */
+int dnspir_fleet_set_wait_limit(dnspir_fleet* fleet, uint64_t wait_ns, int withhold_chunk);
 /* The tensor scan's tile shapes (query-operand rows per CTA, m-tiles per CTA,
  * pipeline stages, 1 for the persistent warp-specialised kernel); returns
  * their count. */
@@ -252,6 +283,11 @@ int dnspir_fleet_batch_timings(dnspir_fleet* fleet, uint32_t max, double* latenc
                                double* secondary_ms, double* scan_ms);
 /* Launch on a caller-owned cudaStream_t (NULL restores the fleet's own stream). */
 int dnspir_fleet_set_stream(dnspir_fleet* fleet, void* cuda_stream);
+/* Kernels the fleet's answer pipeline has launched so far (counted at each
+ * launch: decode, query operand and scan, epilogue, and per secondary chunk the
+ * encoder's three kernels, the chains and the replies).  No counterpart in the
+ * reference. */
+int dnspir_fleet_launch_count(dnspir_fleet* fleet, uint64_t* count);
 /* Bytes of slab memory the fleet holds on its device. */
 uint64_t dnspir_fleet_slab_bytes(dnspir_fleet* fleet);
 int dnspir_fleet_destroy(dnspir_fleet* fleet);

@@ -380,7 +380,11 @@ static inline size_t gal2idx(size_t N, int64_t g) {
 // ----------------------------------------------------------------- BFV (bfv.rs)
 typedef std::vector<int64_t> Poly;  // coefficients in [0, q) (or [0, t))
 
-// expand (bfv.rs:46-49): this project's sampler over the StdRng word stream
+// expand (bfv.rs:46-49): coefficient i = 0..N-1 in turn, each the low
+// ceil(log2 q) = 51 bits of one StdRng next_u64, drawn again while >= q -- the
+// uniform-below-bound rule feanor-math 3.5.18's random_element applies per
+// coefficient, as this project restates it (the crate is not available here to
+// confirm the restatement)
 static Poly expand(size_t N, const uint8_t seed[32]) {
   StdRng rng(seed);
   Poly out(N);
@@ -1314,13 +1318,17 @@ int orc_ms_decode(int bits, const uint64_t* x, uint64_t n, int64_t* out) {
 
 // process_queries (pir_wrapper.rs:349-409) for one query in batch slot 0;
 // fleet = ndb shard handles (shard k of the fleet is dbs[k]).
-int orc_process_query(orc_db** dbs, uint32_t ndb, const uint8_t* query, uint64_t qlen, uint8_t* reply,
-                      uint64_t* reply_len) {
+// process_query with an explicit secondary group order (0: the shape rule's
+// choose_index_group_secondary, pir_wrapper.rs:166-175), as the reference's
+// perform_double_pir allows (double_pir.rs:104-123)
+int orc_process_query_general(orc_db** dbs, uint32_t ndb, uint32_t l2, const uint8_t* query, uint64_t qlen,
+                              uint8_t* reply, uint64_t* reply_len) {
   ORC_TRY({
     const size_t N = (size_t)1 << LOG2_N_WIRE;
     ORC_CHECK(ndb >= 1 && dbs[0]->s.R->n == N, "fleet must be built at N = 2048");
     IndexGroup ig1 = dbs[0]->s.ig;
-    IndexGroup ig2 = choose_secondary(ndb);
+    IndexGroup ig2 = l2 ? make_group(N, l2) : choose_secondary(ndb);
+    ORC_CHECK((size_t)ndb * SIMD <= ig2.l, "secondary group too small for the number of shards");
     size_t pos = 0;
     std::vector<uint64_t> raw(N);
     auto take = [&](int bits) {
@@ -1353,6 +1361,11 @@ int orc_process_query(orc_db** dbs, uint32_t ndb, const uint8_t* query, uint64_t
     memcpy(reply, out.data(), out.size());
     *reply_len = out.size();
   })
+}
+
+int orc_process_query(orc_db** dbs, uint32_t ndb, const uint8_t* query, uint64_t qlen, uint8_t* reply,
+                      uint64_t* reply_len) {
+  return orc_process_query_general(dbs, ndb, 0, query, qlen, reply, reply_len);
 }
 
 // ---- client side (test only)

@@ -86,6 +86,8 @@ def _declare(L):
     L.orc_ms_encode.argtypes = [c.c_int, c.c_void_p, c.c_uint64, c.c_void_p]
     L.orc_ms_decode.argtypes = [c.c_int, c.c_void_p, c.c_uint64, c.c_void_p]
     L.orc_process_query.argtypes = [c.c_void_p, c.c_uint32, c.c_void_p, c.c_uint64, c.c_void_p, _p(c.c_uint64)]
+    L.orc_process_query_general.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32, c.c_void_p, c.c_uint64, c.c_void_p,
+                                            _p(c.c_uint64)]
     L.orc_gen_sk.argtypes = [c.c_void_p, c.c_int, c.c_void_p]
     L.orc_enc_sym_b.argtypes = [c.c_void_p, c.c_int, c.c_int, c.c_void_p, c.c_void_p, c.c_void_p]
     L.orc_gen_gk_b.argtypes = [c.c_void_p, c.c_int, c.c_void_p, c.c_void_p]
@@ -103,6 +105,10 @@ def _declare(L):
         L.orc_cpu_has_avx512.restype = c.c_int
         L.orc_time_secondary.restype = c.c_double
         L.orc_time_secondary.argtypes = [c.c_int, c.c_uint32]
+        L.orc_bench_new.restype = c.c_void_p
+        L.orc_bench_new.argtypes = [c.c_int, c.c_uint32, c.c_uint32, c.c_uint32, c.c_uint32]
+        L.orc_bench_free.argtypes = [c.c_void_p]
+        L.orc_bench_step.argtypes = [c.c_void_p, c.c_int, _p(c.c_double), _p(c.c_double), _p(c.c_int)]
 
 
 class OracleError(RuntimeError):
@@ -154,6 +160,17 @@ def aparts(log2n):
     out = np.zeros((6, 1 << log2n), dtype=np.int64)
     _check(lib().orc_get_aparts(log2n, _ptr(out)))
     return out
+
+
+def set_aparts(log2n, parts):
+    """Replace the six a-parts of dimension 2^log2n ((6, N) in [0, q)); None
+    restores the seed expansion."""
+    if parts is None:
+        _check(lib().orc_set_aparts(log2n, None))
+        return
+    a = np.ascontiguousarray(parts, dtype=np.int64)
+    assert a.shape == (6, 1 << log2n)
+    _check(lib().orc_set_aparts(log2n, _ptr(a)))
 
 
 def expand(log2n, seed):
@@ -280,13 +297,16 @@ def mod_switch_decode(bits, x):
     return out
 
 
-def process_query(dbs, query):
-    """process_query (pir_wrapper.rs:328) on a fleet whose shard k is dbs[k]."""
+def process_query(dbs, query, secondary_order=0):
+    """process_query (pir_wrapper.rs:328) on a fleet whose shard k is dbs[k];
+    secondary_order 0 follows the shape rule (choose_index_group_secondary),
+    else the secondary group has that order (perform_double_pir allows any)."""
     arr = (ctypes.c_void_p * len(dbs))(*[d._h.value for d in dbs])
     q = np.frombuffer(bytes(query), dtype=np.uint8)
     out = np.zeros(1 << 16, dtype=np.uint8)
     n = ctypes.c_uint64()
-    _check(lib().orc_process_query(arr, len(dbs), _ptr(q), len(q), _ptr(out), ctypes.byref(n)))
+    _check(lib().orc_process_query_general(arr, len(dbs), secondary_order, _ptr(q), len(q), _ptr(out),
+                                           ctypes.byref(n)))
     return out[: n.value].tobytes()
 
 
@@ -376,3 +396,27 @@ def time_secondary(log2n, l2):
 
 def cpu_has_avx512():
     return bool(lib().orc_cpu_has_avx512())
+
+
+class QueryBench:
+    """One whole query answered on the CPU, timed for real: the AVX-512
+    main_pir_loop restatement over every logical shard (distinct slabs in RAM
+    reused as shard k mod distinct) plus the oracle's secondary phase."""
+
+    def __init__(self, log2n, l1, l2, shards, distinct):
+        self._h = ctypes.c_void_p(lib().orc_bench_new(log2n, l1, l2, shards, distinct))
+        if not self._h.value:
+            raise OracleError("out of host memory for the CPU bench slabs")
+
+    def step(self, threads=0):
+        """(scan seconds, secondary seconds, scan threads) of one query."""
+        a, b, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().orc_bench_step(self._h, threads, ctypes.byref(a), ctypes.byref(b), ctypes.byref(t)))
+        return a.value, b.value, t.value
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.orc_bench_free(self._h)
+            self._h = None
+
+    __del__ = close

@@ -172,6 +172,113 @@ double orc_scan_baseline(int log2n, uint32_t l, uint32_t shards, int threads, in
   return best;
 }
 
+// ---- one whole query on the CPU, timed for real (the reference arm of the
+// bench): the primary scan of every logical shard (shard k reads distinct slab
+// k mod distinct, as bench_wrapped_pir's preprocessed-db-count does,
+// pir_wrapper.rs:578), run in parallel over (shard, prime, half) units on all
+// threads, then the secondary phase (set_db of the per-query database and its
+// scan, double_pir.rs:195-218) on the oracle.
+struct orc_bench {
+  int log2n = 11;
+  uint32_t l1 = 0, l2 = 0, shards = 0, distinct = 0;
+  size_t N = 0, L = 0, arr = 0;
+  int H = 1;
+  uint32_t* slab = nullptr;  // distinct x 2 primes x H halves x 3 arrays
+  std::vector<uint32_t> qv, gal;
+  std::vector<uint16_t> sec_entries;
+};
+
+orc_bench* orc_bench_new(int log2n, uint32_t l1, uint32_t l2, uint32_t shards, uint32_t distinct) {
+  orc_bench* b = new orc_bench();
+  b->log2n = log2n;
+  b->l1 = l1;
+  b->l2 = l2;
+  b->shards = shards;
+  b->distinct = std::max<uint32_t>(1, std::min(distinct, shards));
+  b->N = (size_t)1 << log2n;
+  b->L = l1 < b->N ? l1 : b->N / 2;
+  b->H = l1 == b->N ? 2 : 1;
+  b->arr = b->L * b->N * 8;
+  const size_t words = (size_t)b->distinct * 2 * b->H * 3 * b->arr;
+  b->slab = (uint32_t*)aligned_alloc(64, words * 4);
+  if (!b->slab) {
+    delete b;
+    return nullptr;
+  }
+  const int nt = std::max(1, (int)std::thread::hardware_concurrency());
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&, t]() {
+      uint64_t x = 0x9e3779b97f4a7c15ull * (t + 1);
+      for (size_t i = (size_t)t * (words / nt); i < (t == nt - 1 ? words : (size_t)(t + 1) * (words / nt)); i++) {
+        x ^= x << 13;
+        x ^= x >> 7;
+        x ^= x << 17;
+        b->slab[i] = (uint32_t)(x % BQ2);
+      }
+    });
+  for (auto& t : th) t.join();
+  b->qv.resize(4 * b->N * 8);
+  for (size_t i = 0; i < b->qv.size(); i++) b->qv[i] = (uint32_t)((i * 2654435761u) % BQ2);
+  b->gal.resize(b->N);
+  for (size_t i = 0; i < b->N; i++) b->gal[i] = (uint32_t)((i * 5 + 3) % b->N);  // any permutation (cost only)
+  b->sec_entries.resize((size_t)8 * l2 * b->N);
+  for (size_t i = 0; i < b->sec_entries.size(); i++) b->sec_entries[i] = (uint16_t)((i * 2654435761u) % 1025);
+  return b;
+}
+
+void orc_bench_free(orc_bench* b) {
+  if (!b) return;
+  free(b->slab);
+  delete b;
+}
+
+// One query: seconds of the primary scan and of the secondary phase.
+// *scan_threads receives the threads that took scan units.
+int orc_bench_step(orc_bench* b, int threads, double* scan_s, double* sec_s, int* scan_threads) {
+  const size_t units = (size_t)b->shards * 2 * b->H;
+  int nt = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+  nt = std::max(1, std::min<int>(nt, (int)units));
+  if (scan_threads) *scan_threads = nt;
+  const bool avx = has_avx512();
+  const size_t per_unit = 3 * b->arr;
+  std::atomic<size_t> next(0);
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&]() {
+      uint64_t* bufs = (uint64_t*)aligned_alloc(64, 2 * b->N * 8 * 8);
+      for (;;) {
+        const size_t k = next.fetch_add(1);
+        if (k >= units) break;
+        // unit k = (logical shard, prime, half); logical shard s reads distinct slab s mod distinct
+        const size_t shard = k / (2 * b->H), ph = k % (2 * b->H);
+        const uint32_t* base = b->slab + ((shard % b->distinct) * 2 * b->H + ph) * per_unit;
+        Unit u{base, base + b->arr, base + 2 * b->arr, b->qv.data(), b->qv.data() + 2 * b->N * 8,
+               b->qv.data() + 3 * b->N * 8, (ph / b->H) % 2 ? BQ2 : BQ1};
+        memset(bufs, 0, 2 * b->N * 8 * 8);
+        if (avx)
+          loop_avx512(u, b->N, b->L, 341, b->gal.data(), (__m512i*)bufs, (__m512i*)(bufs + b->N * 8));
+        else
+          loop_scalar(u, b->N, b->L, 341, b->gal.data(), bufs, bufs + b->N * 8);
+      }
+      free(bufs);
+    });
+  for (auto& t : th) t.join();
+  auto t1 = std::chrono::steady_clock::now();
+  void* db = nullptr;
+  int rc = orc_db_create(b->log2n, b->l2, 1, &db);
+  std::vector<int64_t> q(8 * b->N, 1), gk(16 * b->N, 1), out(8 * b->N);
+  if (!rc) rc = orc_db_set_db(db, b->sec_entries.data());
+  if (!rc) rc = orc_db_get_a(db, out.data());
+  if (!rc) rc = orc_db_perform_pir_split(db, q.data(), b->l2 == b->N ? q.data() : nullptr, gk.data(), out.data());
+  auto t2 = std::chrono::steady_clock::now();
+  if (db) orc_db_free(db);
+  if (scan_s) *scan_s = std::chrono::duration<double>(t1 - t0).count();
+  if (sec_s) *sec_s = std::chrono::duration<double>(t2 - t1).count();
+  return rc;
+}
+
 // Seconds of one secondary phase at N = 2^log2n and secondary order l2:
 // set_db of the per-query database (8 l2 entries) and perform_pir_split.
 double orc_time_secondary(int log2n, uint32_t l2) {

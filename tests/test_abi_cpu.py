@@ -128,3 +128,62 @@ def test_client_reads_oracle_reply():
         assert np.array_equal(dp.process_reply(reply, sk), data[i])
     with pytest.raises(dp.DnspirError):
         dp.process_reply(reply[:-10], sk)
+
+
+def _random_aparts(log2n, seed):
+    return np.random.default_rng(seed).integers(0, dp.Q, size=(6, 1 << log2n), dtype=np.int64).astype(np.uint64)
+
+
+@pytest.mark.parametrize("log2n", [3, 8, 11])
+def test_a_parts_hook_roundtrip(log2n):
+    # dnspir_set_a_parts installs a-parts (e.g. vectors produced by the
+    # reference's expand, bfv.rs:46-49); NULL restores the seed expansion
+    default = dp.get_a_parts(log2n)
+    assert np.array_equal(default, np.stack([dp.expand_seed(log2n, w) for w in range(6)]))
+    mine = _random_aparts(log2n, 5)
+    try:
+        dp.set_a_parts(log2n, mine)
+        assert np.array_equal(dp.get_a_parts(log2n), mine)
+        # the seed expansion itself is unchanged
+        assert np.array_equal(dp.expand_seed(log2n, 0), default[0])
+    finally:
+        dp.set_a_parts(log2n, None)
+    assert np.array_equal(dp.get_a_parts(log2n), default)
+
+
+def test_a_parts_hook_rejects_unreduced(tmp_path):
+    bad = _random_aparts(8, 6)
+    bad[3, 17] = dp.Q
+    with pytest.raises(dp.DnspirError) as e:
+        dp.set_a_parts(8, bad)
+    assert e.value.code == 6
+    assert np.array_equal(dp.get_a_parts(8), np.stack([dp.expand_seed(8, w) for w in range(6)]))
+    # the file form: raw little-endian uint64, 6 x N
+    mine = _random_aparts(8, 7)
+    f = tmp_path / "aparts.bin"
+    mine.astype("<u8").tofile(f)
+    try:
+        dp.load_a_parts_file(str(f), log2_n=8)
+        assert np.array_equal(dp.get_a_parts(8), mine)
+    finally:
+        dp.set_a_parts(8, None)
+
+
+def test_client_uses_installed_a_parts():
+    # with the same a-parts installed in both, the library's client and the
+    # oracle's client write the same query bytes, and those differ from the
+    # default a-parts' query
+    l1, l2, _ = dp.get_database_shape(32768)
+    seed = bytes(range(32))
+    q0, _ = dp.prepare_query(seed, 3, 1, l1, l2)
+    mine = _random_aparts(11, 8)
+    try:
+        dp.set_a_parts(11, mine)
+        orc.set_aparts(11, mine.astype(np.int64))
+        q, sk = dp.prepare_query(seed, 3, 1, l1, l2)
+        q2, sk2 = orc.prepare_query(orc.Rng(seed), 3, 1, l1, l2)
+    finally:
+        dp.set_a_parts(11, None)
+        orc.set_aparts(11, None)
+    assert q == q2 and sk == sk2
+    assert q != q0

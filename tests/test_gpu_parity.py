@@ -315,3 +315,80 @@ def test_full_secondary_group_large_chunk(full_secondary):
         if k in (0, 7, 15):
             assert r == orc.process_query(refs, q), k
         assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), k
+
+
+def _random_aparts(log2n, seed):
+    return np.random.default_rng(seed).integers(0, orc.Q, size=(6, 1 << log2n), dtype=np.int64)
+
+
+def test_installed_a_parts_follow_through_get_a_and_replies():
+    # dnspir_set_a_parts (the hook for a-parts produced by the reference's own
+    # expand, bfv.rs:46-49) and orc_set_aparts with the same six polynomials:
+    # get_a (base_pir.rs:897) and the double-PIR reply follow them identically
+    # on the GPU and in the oracle, differ from the default a-parts' results,
+    # and the replies decrypt; a fleet preprocessed before the change answers
+    # NOT_READY until its shards are set again
+    log2n, n, l1, l2 = 8, 256, 256, 32
+    data, refs, fleet = _fleets(log2n, l1, l2, 4, 2, 61)
+    db = dp.PIRDatabase(log2n, l1)
+    db.set_db(data[0])
+    a_default = db.get_a().astype(np.int64)
+    mine = _random_aparts(log2n, 62)
+    try:
+        dp.set_a_parts(log2n, mine.astype(np.uint64))
+        orc.set_aparts(log2n, mine)
+        with pytest.raises(dp.DnspirError) as e:
+            db.get_a()
+        assert e.value.code == 7
+        rng = orc.Rng(bytes([63]) + bytes(31))
+        sk = orc.gen_sk(rng, log2n)
+        pq, pqc, sq, sqc, gk = orc.enc_double_pir(rng, log2n, l1, l2, sk, 77, 3)
+        with pytest.raises(dp.DnspirError) as e:
+            fleet.perform_double_pir(pq, pqc, sq, sqc, gk)
+        assert e.value.code == 7
+        db.set_db(data[0])
+        ref0 = orc.Database(log2n, l1)
+        ref0.set_db(data[0])
+        a_mine = db.get_a().astype(np.int64)
+        assert np.array_equal(a_mine, ref0.get_a())
+        assert not np.array_equal(a_mine, a_default)
+        fleet.set_shards(0, data)
+        refs2 = []
+        for k in range(2):
+            d = orc.Database(log2n, l1)
+            d.set_db(data[k])
+            refs2.append(d)
+        want = orc.perform_double_pir([refs2[k % 2] for k in range(4)], l2, pq, pqc, sq, sqc, gk)
+        got = fleet.perform_double_pir(pq, pqc, sq, sqc, gk).astype(np.int64)
+        assert np.array_equal(got, want)
+        assert np.array_equal(orc.dec_double_pir(log2n, sk, got.reshape(6, n)), data[1][77].astype(np.int64))
+    finally:
+        dp.set_a_parts(log2n, None)
+        orc.set_aparts(log2n, None)
+    db.set_db(data[0])
+    assert np.array_equal(db.get_a().astype(np.int64), a_default)
+    fleet.close()
+
+
+def test_installed_a_parts_wire_path_at_n2048():
+    # the byte-level path (process_query, pir_wrapper.rs:328) at N = 2048 under
+    # installed a-parts: the library's client writes the oracle client's bytes,
+    # the GPU reply equals the oracle's and decrypts
+    mine = _random_aparts(11, 64)
+    l1, l2 = 1024, 32
+    try:
+        dp.set_a_parts(11, mine.astype(np.uint64))
+        orc.set_aparts(11, mine)
+        data, refs, fleet = _fleets(11, l1, l2, 4, 2, 65)
+        for (i, j) in [(3, 0), (8000, 3)]:
+            seed = bytes([66, i % 256, j]) + bytes(29)
+            q, sk = dp.prepare_query(seed, i, j, l1, l2)
+            q2, sk2 = orc.prepare_query(orc.Rng(seed), i, j, l1, l2)
+            assert q == q2 and sk == sk2
+            r = fleet.process_query(q)
+            assert r == orc.process_query(refs, q)
+            assert np.array_equal(dp.process_reply(r, sk), data[j % 2][i])
+        fleet.close()
+    finally:
+        dp.set_a_parts(11, None)
+        orc.set_aparts(11, None)

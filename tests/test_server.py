@@ -126,3 +126,29 @@ def test_server_rejects_and_detaches(two_dbs):
         sv.stop()
         sv.close()
     assert r == fa.process_query(q)  # detached again
+
+
+def test_wait_times_out_and_the_request_is_still_answered(two_dbs):
+    # dnspir_server_wait's host timeout: a request held back by a long batching
+    # window (16 queries or 300 ms) is not answered within 1 ms; the wait
+    # returns DNSPIR_ERR_TIMEOUT and leaves the ticket in place, and a later
+    # wait receives the reply (the oracle's bytes, decrypting to the entry)
+    (fa, data, refs, shape), _ = two_dbs
+    sv = dp.Server(device=0)
+    try:
+        db = sv.add_db(fa, 16)
+        sv.set_batching(db, 16, 300.0)
+        sv.start(graphs=False)
+        q, seed, i, j = _queries(shape, 1, 91)[0]
+        t0 = time.perf_counter()
+        ticket = sv.submit(db, q)
+        with pytest.raises(dp.DnspirError) as e:
+            sv.wait(ticket, timeout_ms=1)
+        assert e.value.code == 5
+        r = sv.wait(ticket, timeout_ms=120000)
+        assert time.perf_counter() - t0 >= 0.25  # it waited for the window
+        assert r == orc.process_query(refs, q)
+        assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64))
+    finally:
+        sv.stop()
+        sv.close()

@@ -214,3 +214,30 @@ def test_empty_call_and_largest_group(config1_pair):
         if k % 37 == 0 or k == 255:
             assert r == orc.process_query(refs, q), k
         assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), k
+
+
+@pytest.mark.parametrize("persistent", [0, 1, 2])
+def test_scan_wait_runs_out_and_the_device_stays_usable(persistent):
+    # the timeout path of the tensor scan's bounded waits: with a 2 ms limit
+    # and the first block's producer withholding one chunk, that block's MMA
+    # thread gives up, the block drains its copies, frees its tensor memory and
+    # returns; the call fails with DNSPIR_ERR_TIMEOUT.  The next call, with the
+    # default limit and nothing withheld, answers correctly.
+    torch = pytest.importorskip("torch")
+    n = 256
+    _, fa, fb = _pair(8, 256, 256, 1, 1, 77)
+    if persistent:
+        # the persistent one-CTA kernel, or the CTA-pair kernel (whose leader
+        # then gives up and raises the pair's abort flag for its follower)
+        shapes = dp.tscan_shapes()
+        fb.set_tile(1, next(i for i, s in enumerate(shapes) if s[3] == persistent))
+    q = _qnat(torch, 1, n, 78)
+    want = _scan(torch, fa, q, 1, n)
+    fb.set_wait_limit(2_000_000, withhold_chunk=2)
+    with pytest.raises(dp.DnspirError) as e:
+        _scan(torch, fb, q, 1, n)
+    assert e.value.code == 5
+    fb.set_wait_limit()
+    assert np.array_equal(_scan(torch, fb, q, 1, n), want)
+    fa.close()
+    fb.close()
