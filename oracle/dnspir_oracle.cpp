@@ -369,7 +369,7 @@ static IndexGroup make_group(size_t N, size_t l) {
   return IndexGroup{N, l};
 }
 // index_to_galois / galois_to_index with group_order = N (base_pir.rs:185-191)
-static inline int64_t idx2gal(size_t N, int64_t i) { return 2 * i + 1; }
+static inline int64_t idx2gal(size_t /*N*/, int64_t i) { return 2 * i + 1; }
 static inline size_t gal2idx(size_t N, int64_t g) {
   int64_t m = 2 * (int64_t)N;
   int64_t x = mod_floor(g, m);
