@@ -8,17 +8,17 @@ Each case is one database of a single non-zero entry (1 or X at entry
 store, as coefficients in {0, 1, -1} before the factor 1 / `factor` mod t and
 the transform that assert_correctly_preprocessed applies (base_pir.rs:1292-1304).
 
-Run where the reference sources are (REF below, or DNSPIR_REFERENCE); the JSON
-is committed and the tests read only the JSON:
+Run with DNSPIR_REFERENCE naming a checkout of the reference (the directory
+holding crates/pir); the JSON is committed and the tests read only the JSON:
 
-    python tests/golden/make_golden.py
+    DNSPIR_REFERENCE=<path to the reference checkout> python tests/golden/make_golden.py
 """
 import json
 import os
 import re
 
-REF = os.environ.get("DNSPIR_REFERENCE", "/root/reference")
-SRC = os.path.join(REF, "crates", "pir", "src", "base_pir.rs")
+REF = os.environ.get("DNSPIR_REFERENCE")
+SRC = os.path.join(REF or "", "crates", "pir", "src", "base_pir.rs")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kat_layout_n8.json")
 TESTS = ("test_set_transformed_entries_full_group", "test_set_transformed_entries_full_g_subgroup",
          "test_set_transformed_entries_small_subgroup")
@@ -37,6 +37,8 @@ def parse_rows(text):
 
 
 def main():
+    if not REF:
+        raise SystemExit("set DNSPIR_REFERENCE to the reference checkout (the directory holding crates/pir)")
     src = open(SRC).read()
     out = {"source": "crates/pir/src/base_pir.rs:1281-1411", "t": 1025, "tests": {}}
     for name in TESTS:
