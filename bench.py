@@ -620,10 +620,12 @@ def main():
     slab_bytes = dp.required_memory_general(11, l1) * 32
     free, _ = torch.cuda.mem_get_info()
     sizes = [int(x) for x in args.batched.split(",") if x.strip()]
-    # workspaces: two buffer slots of scan output for the largest group, the
-    # secondary phase's chunk (at most 6 GiB) and headroom
+    # workspaces: two buffer slots, each with the scan output and the
+    # secondary input of the largest group, the secondary phase's chunk (at
+    # most 6 GiB) and headroom
+    per_query_ws = shards * 2 * dp.N * 8 * 4 + l2 * 3 * dp.N * 2
     reserve = args.reserve_gib * (1 << 30) if args.reserve_gib > 0 else \
-        2 * max(sizes + [1]) * shards * 2 * dp.N * 8 * 4 + (14 << 30)
+        2 * max(sizes + [1]) * per_query_ws + (10 << 30)
     fit = int((free - int(reserve)) // slab_bytes)
     distinct = args.distinct if args.distinct > 0 else max(1, min(shards, fit))
 

@@ -110,15 +110,25 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
+// TMEM columns taddr .. taddr + 15 of this warp's 32 lanes; the wait is in the
+// same asm statement, so no use of v can be scheduled before the data is there
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr)
       : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+// TMEM columns taddr .. taddr + 63 of this warp's 32 lanes; the wait is in the
+// same asm statement, so no use of v can be scheduled before the data is there
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]), "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]), "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]), "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]), "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+      : "r"(taddr)
+      : "memory");
 }
 
 struct TScanArgs {
@@ -133,6 +143,56 @@ struct TScanArgs {
   uint64_t wait_ns;   // limit of every pipeline wait
   uint32_t withhold;  // test hook: CTA 0's producer stops before this chunk (~0u: never)
 };
+
+// c_w = 2^(8w) mod p (< 2^26) for w = k .. k + 3: the weights of limb product
+// D_kj (j = 0..3) in the recombination
+__device__ __forceinline__ void limb_weights(uint32_t pr, uint64_t mu, int k, uint32_t (&c)[4]) {
+  const uint32_t w3 = (uint32_t)reduce64(1ull << 24, pr, mu);
+  const uint64_t c32 = reduce64(1ull << 32, pr, mu);
+  const uint64_t c40 = reduce64(c32 << 8, pr, mu);
+  const uint64_t c48 = reduce64(c40 << 8, pr, mu);
+  c[0] = k == 0 ? 1u : k == 1 ? 256u : k == 2 ? 65536u : w3;
+  c[1] = k == 0 ? 256u : k == 1 ? 65536u : k == 2 ? w3 : (uint32_t)c32;
+  c[2] = k == 0 ? 65536u : k == 1 ? w3 : k == 2 ? (uint32_t)c32 : (uint32_t)c40;
+  c[3] = k == 0 ? w3 : k == 1 ? (uint32_t)c32 : k == 2 ? (uint32_t)c40 : (uint32_t)c48;
+}
+
+// Epilogue of one m-tile: the warp's 32 TMEM lanes (rows (slot, lane, limb k)
+// of output slot u) x NQ columns (query-operand rows 4 b + j of query group
+// grp) starting at TMEM address taddr.  Each query's 16 limb products are
+// recombined with the weights c and reduced mod pr; lanes 4 l8 .. 4 l8 + 3
+// hold the four limbs k of SIMD lane l8, so three of every four lanes sum the
+// others' partial recombinations with shuffles and lane k keeps query
+// 4 q4 + k's sum.  Columns are read 64 (16 for NQ = 16) per TMEM load.
+template <int NQ>
+__device__ __forceinline__ void epilogue_tile(const TScanArgs& a, uint32_t taddr, const uint32_t (&c)[4], uint32_t pr,
+                                              uint64_t mu, uint32_t grp, uint32_t u, int s, int p, int k, int l8) {
+  constexpr int CW = NQ >= 64 ? 64 : 16;  // columns per TMEM load
+  const uint32_t N = 2 * a.half;
+#pragma unroll 1
+  for (int c0 = 0; c0 < NQ; c0 += CW) {
+    uint32_t v[CW];
+    if constexpr (CW == 64)
+      tmem_ld64(taddr + c0, v);
+    else
+      tmem_ld16(taddr + c0, v);
+#pragma unroll
+    for (int q4 = 0; q4 < CW / 16; q4++) {
+      uint64_t tot[4];
+#pragma unroll
+      for (int qq = 0; qq < 4; qq++) {
+        const uint32_t* w = v + 16 * q4 + 4 * qq;
+        uint64_t x = (uint64_t)w[0] * c[0] + (uint64_t)w[1] * c[1] + (uint64_t)w[2] * c[2] + (uint64_t)w[3] * c[3];
+        x += __shfl_xor_sync(0xffffffffu, x, 1);
+        x += __shfl_xor_sync(0xffffffffu, x, 2);
+        tot[qq] = x;
+      }
+      const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
+      const uint32_t bq = grp * (NQ / 4) + (c0 / 16 + q4) * 4 + k;
+      if (bq < a.nvalid) a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
+    }
+  }
+}
 
 template <int NQ, int MTPC>
 __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
@@ -243,41 +303,12 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
   if (acc_ok) {
     const uint32_t pr = prime_of(p);
     const uint64_t mu = barrett_mu(pr);
-    uint64_t cw[7];
-    cw[0] = 1;
-    cw[1] = 256;
-    cw[2] = 65536;
-    cw[3] = reduce64(1ull << 24, pr, mu);
-    cw[4] = reduce64(1ull << 32, pr, mu);
-    cw[5] = reduce64(cw[4] << 8, pr, mu);
-    cw[6] = reduce64(cw[5] << 8, pr, mu);
     const int k = lane & 3, l8 = lane >> 2;
-    const uint32_t c0 = (uint32_t)(k == 0 ? cw[0] : k == 1 ? cw[1] : k == 2 ? cw[2] : cw[3]);
-    const uint32_t c1 = (uint32_t)(k == 0 ? cw[1] : k == 1 ? cw[2] : k == 2 ? cw[3] : cw[4]);
-    const uint32_t c2 = (uint32_t)(k == 0 ? cw[2] : k == 1 ? cw[3] : k == 2 ? cw[4] : cw[5]);
-    const uint32_t c3 = (uint32_t)(k == 0 ? cw[3] : k == 1 ? cw[4] : k == 2 ? cw[5] : cw[6]);  // 2^(8w) mod p < 2^26
-    const uint32_t N = 2 * a.half;
-    for (int t = 0; t < MTPC; t++) {
-      const uint32_t u = sgn * a.half + 4 * (mt0 + t) + warp;
-#pragma unroll 1
-      for (int q4 = 0; q4 < NQ / 16; q4++) {
-        uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + t * NQ + 16 * q4, v);
-        uint64_t tot[4];
-#pragma unroll
-        for (int qq = 0; qq < 4; qq++) {
-          uint64_t x = (uint64_t)v[4 * qq] * c0 + (uint64_t)v[4 * qq + 1] * c1 + (uint64_t)v[4 * qq + 2] * c2 +
-                       (uint64_t)v[4 * qq + 3] * c3;
-          x += __shfl_xor_sync(0xffffffffu, x, 1);
-          x += __shfl_xor_sync(0xffffffffu, x, 2);
-          tot[qq] = x;
-        }
-        const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
-        const uint32_t bq = grp * (NQ / 4) + 4 * q4 + k;
-        if (bq < a.nvalid)
-          a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
-      }
-    }
+    uint32_t c[4];
+    limb_weights(pr, mu, k, c);
+    for (int t = 0; t < MTPC; t++)
+      epilogue_tile<NQ>(a, tmem + ((uint32_t)(32 * warp) << 16) + t * NQ, c, pr, mu, grp,
+                        sgn * a.half + 4 * (mt0 + t) + warp, s, p, k, l8);
   } else if (threadIdx.x == 0) {
     atomicOr(a.err, 1u);
   }
@@ -315,7 +346,10 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
   constexpr uint32_t A_BYTES = MTPC * TBLK;
   constexpr uint32_t STAGE = A_BYTES + NQ * 128;
   constexpr uint32_t ACC = MTPC * NQ;  // TMEM columns of one accumulator
-  constexpr uint32_t COLS = 2 * ACC;
+  // two accumulators when they fit the SM's 512 columns; with one, the MMAs of
+  // a tile wait for the previous tile's epilogue, but its chunks still stream in
+  constexpr uint32_t BUFS = 2 * ACC <= 512 ? 2 : 1;
+  constexpr uint32_t COLS = BUFS * ACC;
   static_assert(STAGE % 1024 == 0 && ACC >= 16 && COLS <= 512 && (COLS & (COLS - 1)) == 0, "tile shape");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -407,7 +441,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
       constexpr uint32_t idesc = idesc_u8(128, NQ);
       uint32_t g = 0, j = 0;
       for (uint32_t item = blockIdx.x; item < items && !*abort_s; item += gridDim.x, j++) {
-        const uint32_t buf = j & 1, use = j >> 1;
+        const uint32_t buf = j % BUFS, use = j / BUFS;
         if (use > 0 && !mbar_wait(&acce[buf], (use - 1) & 1, a.wait_ns)) {
           *abort_s = 1;
           atomicOr(a.err, 1u);
@@ -442,10 +476,9 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
   } else {
     const int q = warp & 3;  // TMEM lane quarter = slot e mod 4 of the m-tile
     const int k = lane & 3, l8 = lane >> 2;
-    const uint32_t N = 2 * a.half;
     uint32_t j = 0;
     for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, j++) {
-      const uint32_t buf = j & 1, use = j >> 1;
+      const uint32_t buf = j % BUFS, use = j / BUFS;
       if (!mbar_wait(&accf[buf], use & 1, a.wait_ns)) {
         if (lane == 0) {
           *abort_s = 1;
@@ -459,36 +492,11 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
       tile_of(item, grp, mt0, sgn, p, s);
       const uint32_t pr = prime_of(p);
       const uint64_t mu = barrett_mu(pr);
-      const uint64_t c32 = reduce64(1ull << 32, pr, mu);
-      const uint64_t c40 = reduce64(c32 << 8, pr, mu);
-      const uint64_t c48 = reduce64(c40 << 8, pr, mu);
-      // c_w = 2^(8w) mod p < 2^26 for w = k .. k + 3
-      const uint32_t w3 = (uint32_t)reduce64(1ull << 24, pr, mu);
-      const uint32_t c0 = k == 0 ? 1u : k == 1 ? 256u : k == 2 ? 65536u : w3;
-      const uint32_t c1 = k == 0 ? 256u : k == 1 ? 65536u : k == 2 ? w3 : (uint32_t)c32;
-      const uint32_t c2 = k == 0 ? 65536u : k == 1 ? w3 : k == 2 ? (uint32_t)c32 : (uint32_t)c40;
-      const uint32_t c3 = k == 0 ? w3 : k == 1 ? (uint32_t)c32 : k == 2 ? (uint32_t)c40 : (uint32_t)c48;
-      for (int t = 0; t < MTPC; t++) {
-        const uint32_t u = sgn * a.half + 4 * (mt0 + t) + q;
-#pragma unroll 1
-        for (int q4 = 0; q4 < NQ / 16; q4++) {
-          uint32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ + 16 * q4, v);
-          uint64_t tot[4];
-#pragma unroll
-          for (int qq = 0; qq < 4; qq++) {
-            uint64_t x = (uint64_t)v[4 * qq] * c0 + (uint64_t)v[4 * qq + 1] * c1 + (uint64_t)v[4 * qq + 2] * c2 +
-                         (uint64_t)v[4 * qq + 3] * c3;
-            x += __shfl_xor_sync(0xffffffffu, x, 1);
-            x += __shfl_xor_sync(0xffffffffu, x, 2);
-            tot[qq] = x;
-          }
-          const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
-          const uint32_t bq = grp * (NQ / 4) + 4 * q4 + k;
-          if (bq < a.nvalid)
-            a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
-        }
-      }
+      uint32_t c[4];
+      limb_weights(pr, mu, k, c);
+      for (int t = 0; t < MTPC; t++)
+        epilogue_tile<NQ>(a, tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ, c, pr, mu, grp,
+                          sgn * a.half + 4 * (mt0 + t) + q, s, p, k, l8);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[buf]);
@@ -751,7 +759,6 @@ __global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
   } else {
     const int q = warp & 3;  // TMEM lane quarter = slot e mod 4 of the m-tile
     const int k = lane & 3, l8 = lane >> 2;
-    const uint32_t N = 2 * a.half;
     const uint32_t acce_leader = peer_addr(&acce[0], 0);
     uint32_t j = 0;
     for (uint32_t item = cid; item < items; item += ncl, j++) {
@@ -766,35 +773,11 @@ __global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
       tile_of(item, grp, mt0, sgn, p, s);
       const uint32_t pr = prime_of(p);
       const uint64_t mu = barrett_mu(pr);
-      const uint64_t c32 = reduce64(1ull << 32, pr, mu);
-      const uint64_t c40 = reduce64(c32 << 8, pr, mu);
-      const uint64_t c48 = reduce64(c40 << 8, pr, mu);
-      const uint32_t w3 = (uint32_t)reduce64(1ull << 24, pr, mu);
-      const uint32_t c0 = k == 0 ? 1u : k == 1 ? 256u : k == 2 ? 65536u : w3;
-      const uint32_t c1 = k == 0 ? 256u : k == 1 ? 65536u : k == 2 ? w3 : (uint32_t)c32;
-      const uint32_t c2 = k == 0 ? 65536u : k == 1 ? w3 : k == 2 ? (uint32_t)c32 : (uint32_t)c40;
-      const uint32_t c3 = k == 0 ? w3 : k == 1 ? (uint32_t)c32 : k == 2 ? (uint32_t)c40 : (uint32_t)c48;
-      for (int t = 0; t < MTPC; t++) {
-        const uint32_t u = sgn * a.half + 4 * (mt0 + rank * MTPC + t) + q;
-#pragma unroll 1
-        for (int q4 = 0; q4 < NQ / 16; q4++) {
-          uint32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ + 16 * q4, v);
-          uint64_t tot[4];
-#pragma unroll
-          for (int qq = 0; qq < 4; qq++) {
-            uint64_t x = (uint64_t)v[4 * qq] * c0 + (uint64_t)v[4 * qq + 1] * c1 + (uint64_t)v[4 * qq + 2] * c2 +
-                         (uint64_t)v[4 * qq + 3] * c3;
-            x += __shfl_xor_sync(0xffffffffu, x, 1);
-            x += __shfl_xor_sync(0xffffffffu, x, 2);
-            tot[qq] = x;
-          }
-          const uint64_t mine = k == 0 ? tot[0] : k == 1 ? tot[1] : k == 2 ? tot[2] : tot[3];
-          const uint32_t bq = grp * (NQ / 4) + 4 * q4 + k;
-          if (bq < a.nvalid)
-            a.out[((((size_t)bq * a.nshards + s) * 2 + p) * N + u) * SIMD + l8] = reduce64(mine, pr, mu);
-        }
-      }
+      uint32_t c[4];
+      limb_weights(pr, mu, k, c);
+      for (int t = 0; t < MTPC; t++)
+        epilogue_tile<NQ>(a, tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ, c, pr, mu, grp,
+                          sgn * a.half + 4 * (mt0 + rank * MTPC + t) + q, s, p, k, l8);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) {
@@ -923,7 +906,7 @@ int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
   const size_t smem = 1024 + (size_t)stages * STAGE + (2 * stages + 5) * 8 + 16;
   if (smem > 227 * 1024) return -1;
   set_smem(tscanp_kernel<NQ, MTPC>, smem);
-  constexpr int COLS = 2 * MTPC * NQ;
+  constexpr int COLS = (2 * MTPC * NQ <= 512 ? 2 : 1) * MTPC * NQ;
   int per_sm = 0, dev = 0, sms = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tscanp_kernel<NQ, MTPC>, TSCANP_NT, smem);
   // resident CTAs must not ask for more TMEM columns than the SM has (a CTA
@@ -999,7 +982,7 @@ const TScanShape* tscan_shapes(int* count) {
       {16, 1, 5, 0},  {16, 1, 10, 0}, {32, 1, 5, 0},  {64, 1, 4, 0},  {64, 2, 3, 0},  {64, 2, 2, 0},
       {128, 1, 3, 0}, {128, 2, 2, 0}, {128, 2, 3, 0}, {256, 1, 2, 0}, {256, 1, 3, 0}, {256, 1, 4, 0},
       {256, 2, 2, 0}, {256, 2, 3, 0}, {512, 1, 2, 0}, {16, 1, 6, 1},  {64, 1, 5, 1},  {64, 2, 4, 1},
-      {128, 1, 4, 1}, {128, 2, 3, 1}, {256, 1, 3, 1}, {256, 1, 4, 1},
+      {128, 1, 4, 1}, {128, 2, 3, 1}, {256, 1, 3, 1}, {256, 1, 4, 1}, {256, 2, 3, 1},
       // CTA pairs (tcgen05.mma.cta_group::2): rows are the pair's query
       // operand rows (each CTA stages half of them)
       {64, 1, 8, 2},  {128, 1, 6, 2}, {128, 2, 4, 2}, {256, 1, 6, 2}, {256, 2, 4, 2},
@@ -1059,6 +1042,7 @@ int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, s
       case 1281: return launch_tp<128, 1>(a, stg, st);
       case 1282: return launch_tp<128, 2>(a, stg, st);
       case 2561: return launch_tp<256, 1>(a, stg, st);
+      case 2562: return launch_tp<256, 2>(a, stg, st);
       default: return -1;
     }
   }
