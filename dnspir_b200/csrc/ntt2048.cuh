@@ -119,10 +119,22 @@ struct ScaleStore {
   }
 };
 
+// Ends a pass: SYNC = 0 synchronises the block; SYNC = 1 only the 256-thread
+// group of the calling thread (named barrier 1 + threadIdx.x / 256), for
+// blocks of 512 threads whose two halves work on one polynomial each.
+template <int SYNC>
+__device__ __forceinline__ void pass_sync() {
+  if constexpr (SYNC == 0) {
+    __syncthreads();
+  } else {
+    asm volatile("bar.sync %0, 256;" ::"r"(1 + (threadIdx.x >> 8)) : "memory");
+  }
+}
+
 // One radix-8 pass over polynomials [0, cnt0) (factor 0) and [cnt0, cnt0 +
 // cnt1) (factor 1) of x.  INV selects Gentleman-Sande with the iw tables; FIN
 // (inverse, M = 1 only) receives the finished values instead of a store.
-template <int NT, int M, bool INV, class Fin>
+template <int NT, int M, bool INV, int SYNC = 0, class Fin>
 __device__ __forceinline__ void pass8(uint32_t* x, int cnt0, int cnt1, const NttTables& T, const Fin& fin) {
   using S = Split<NT, 256>;
   using Gm = Geo8<M>;
@@ -138,7 +150,11 @@ __device__ __forceinline__ void pass8(uint32_t* x, int cnt0, int cnt1, const Ntt
       if (lo >= hi) continue;
       const uint32_t p = prime_of(pi);
       const Tw8 t = load_tw8(INV ? T.iw2[pi] : T.fw2[pi], M, blk);
-      for (int poly = lo + po; poly < hi; poly += S::PPI) {
+      // polynomials are dealt to the PPI thread groups by their global index
+      // (poly mod PPI), so one polynomial per factor still spreads over all
+      // groups
+      const int first = lo + ((po - lo) % S::PPI + S::PPI) % S::PPI;
+      for (int poly = first; poly < hi; poly += S::PPI) {
         uint32_t* y = x + poly * PS + base;
         uint32_t v[8];
 #pragma unroll
@@ -157,7 +173,7 @@ __device__ __forceinline__ void pass8(uint32_t* x, int cnt0, int cnt1, const Ntt
       }
     }
   }
-  __syncthreads();
+  pass_sync<SYNC>();
 }
 
 // Radix-4 pass on the aligned quads 4g .. 4g + 3 (forward stages 9-10 with
@@ -178,7 +194,8 @@ __device__ __forceinline__ void pass4(uint32_t* x, int cnt0, int cnt1, const Ntt
       const uint32_t p = prime_of(pi);
       const Tw4 tw = load_tw4(INV ? T.iw2[pi] : T.fw2[pi], g);
       const uint32_t a = tw.a, aq = tw.aq, b0 = tw.b0, b0q = tw.b0q, b1 = tw.b1, b1q = tw.b1q;
-      for (int poly = lo + po; poly < hi; poly += S::PPI) {
+      const int first = lo + ((po - lo) % S::PPI + S::PPI) % S::PPI;
+      for (int poly = first; poly < hi; poly += S::PPI) {
         uint4* y = reinterpret_cast<uint4*>(x + poly * PS + base);
         uint4 v = *y;
         if (INV) {
