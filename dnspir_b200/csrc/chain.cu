@@ -706,148 +706,172 @@ __device__ __forceinline__ void secondary_dual_body(const ChainArgs& a, int h, i
 }
 
 // ---- N = 2048: one block per part and half carrying both factors, on the
-// register transforms of ntt2048.cuh.  The state a, b stays in natural
-// position order: instead of scattering the next step's sigma_5(a), sigma_5(b)
-// (which needs a second buffer of each), every step gathers them at its own
-// positions through the inverse of galb.  Thread t owns positions 4t .. 4t + 3
-// of both factors in the first inverse pass, the last forward pass and the
-// pointwise stage, so those run from registers; between the last inverse pass
-// and the first forward pass the two factors' threads of a butterfly group
-// swap their values once and both take the high digit.  Eight barriers a step.
-// Shared memory, padded polynomials of n2k::PS words: A[2] (a; also the
-// forward transform's work space), B[2] (b), D[2] (inverse work space).
-constexpr int SEC2K_WORDS = 6 * n2k::PS;
+// register transforms of ntt2048.cuh.  The block's two 256-thread halves
+// work one RNS factor each: half f holds factor f's polynomials in every pass,
+// and thread t of a half owns positions 8t .. 8t + 7 of its factor in the
+// first inverse pass, the last forward pass and the pointwise stage, so those
+// run from registers.  The halves meet once a step: between the last inverse
+// pass and the first forward pass each takes the other's values at its
+// positions for the CRT high digit (the one block-wide barrier); every other
+// barrier is a named barrier of one half.  The inverse work space D is double
+// buffered by step parity, so a half may run a step ahead of the other's reads
+// of its last inverse pass.  The state a, b stays in natural position order:
+// instead of scattering the next step's sigma_5(a), sigma_5(b) (which needs a
+// second buffer of each), every step gathers them at its own positions through
+// the inverse of galb.  Shared memory, padded polynomials of n2k::PS words:
+// A[2] (a; also the forward transform's work space), B[2] (b), D[2][2]; then
+// the six key constants (Montgomery form) of every position, [j][factor]
+// [quad half][thread] as 16-byte vectors, each thread reading only its own.
+constexpr int SEC2K_KC_WORDS = 6 * 2 * 2 * 256 * 4;
+constexpr int SEC2K_WORDS = 8 * n2k::PS + SEC2K_KC_WORDS;
+
+__device__ __forceinline__ void half_sync() {
+  asm volatile("bar.sync %0, 256;" ::"r"(1 + (threadIdx.x >> 8)) : "memory");
+}
 
 __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
   extern __shared__ __align__(16) uint32_t sm[];
   using namespace n2k;
-  static_assert(CT == 512 && N_MAX == N, "one quad per thread and factor");
+  static_assert(CT == 512 && N_MAX == N, "two quads per thread of one factor");
   const int h = blockIdx.x % a.g.H, part = blockIdx.x / a.g.H, q = blockIdx.y;
   uint32_t* const A = sm;
   uint32_t* const B = sm + 2 * PS;
-  uint32_t* const D = sm + 4 * PS;
+  uint32_t* const D = sm + 4 * PS;  // [parity][factor]
   const int tid = threadIdx.x;
-  const int qb = (int)phys(4 * tid);  // this thread's quad
-  const uint32_t pr[2] = {a.cp[0].p, a.cp[1].p};
-  // sigma_5 sources of the quad (galb inverted through D), a = b = 0
+  const int f = tid >> 8, t = tid & 255;  // factor of this half, thread within the half
+  const int qb = (int)phys(8 * t);       // positions 8t .. 8t + 7 sit in one padded row: qb .. qb + 7
+  const ChainPrime cp = f ? a.cp[1] : a.cp[0];
+  const uint32_t p = cp.p;
+  // sigma_5 sources of the positions (galb inverted through D), a = b = 0
   for (int b = tid; b < N; b += CT) D[__ldg(a.galb + b)] = b;
   for (int b = tid; b < 4 * PS; b += CT) sm[b] = 0;
   __syncthreads();
-  uint32_t src[4];
+  uint32_t src[4];  // two 16-bit padded positions per word (PS < 2^16)
 #pragma unroll
-  for (int m = 0; m < 4; m++) src[m] = phys(D[4 * tid + m]);
+  for (int m = 0; m < 4; m++) src[m] = phys(D[8 * t + 2 * m]) | (phys(D[8 * t + 2 * m + 1]) << 16);
   const uint32_t* qq = a.qv + (size_t)q * a.qv_stride;
-  uint32_t kc[2][6][4];
+  uint4* const KC = reinterpret_cast<uint4*>(sm + 8 * PS);  // [j][factor][quad half][t]
 #pragma unroll
-  for (int f = 0; f < 2; f++) {
-    const ChainPrime& cp = a.cp[f];
+  for (int h4 = 0; h4 < 2; h4++) {
+    uint32_t kc[6][4];
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-      const size_t o = (size_t)f * N + 4 * tid + m;
-      kc[f][0][m] = mont_reduce((uint64_t)a.gka[o] * cp.r2, cp.p, cp.pinv);
-      kc[f][1][m] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
-      kc[f][2][m] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, cp.p, cp.pinv);
-      kc[f][3][m] = mont_reduce((uint64_t)qq[o] * cp.r2, cp.p, cp.pinv);
-      kc[f][4][m] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
-      kc[f][5][m] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+      const size_t o = (size_t)f * N + 8 * t + 4 * h4 + m;
+      kc[0][m] = mont_reduce((uint64_t)a.gka[o] * cp.r2, cp.p, cp.pinv);
+      kc[1][m] = mont_reduce((uint64_t)a.gka[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
+      kc[2][m] = mont_reduce((uint64_t)a.qa[(size_t)h * 2 * N + o] * cp.r2, cp.p, cp.pinv);
+      kc[3][m] = mont_reduce((uint64_t)qq[o] * cp.r2, cp.p, cp.pinv);
+      kc[4][m] = mont_reduce((uint64_t)qq[2 * (size_t)N + o] * cp.r2, cp.p, cp.pinv);
+      kc[5][m] = mont_reduce((uint64_t)qq[(size_t)(4 + h) * 2 * N + o] * cp.r2, cp.p, cp.pinv);
       // with t = sigma_5(a): NTT(d0) gk0 + NTT(d1) gk1 = t gk0 + NTT(d1) (gk1 - 2^26 gk0),
       // and likewise for the b-part keys, so the pointwise stage needs no d0
-      kc[f][1][m] = sub_mod(kc[f][1][m], mont_reduce((uint64_t)kc[f][0][m] * cp.c26, cp.p, cp.pinv), cp.p);
-      kc[f][4][m] = sub_mod(kc[f][4][m], mont_reduce((uint64_t)kc[f][3][m] * cp.c26, cp.p, cp.pinv), cp.p);
+      kc[1][m] = sub_mod(kc[1][m], mont_reduce((uint64_t)kc[0][m] * cp.c26, cp.p, cp.pinv), cp.p);
+      kc[4][m] = sub_mod(kc[4][m], mont_reduce((uint64_t)kc[3][m] * cp.c26, cp.p, cp.pinv), cp.p);
     }
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+      KC[((j * 2 + f) * 2 + h4) * 256 + t] = make_uint4(kc[j][0], kc[j][1], kc[j][2], kc[j][3]);
   }
   __syncthreads();  // the table in D is overwritten by the first step
   const size_t lane = (size_t)q * CTXT_PARTS + part;
+  const uint4* Erow = reinterpret_cast<const uint4*>(a.E + (((size_t)f * a.g.H + h) * a.g.L * a.nl + lane) * N);
+  const size_t erow_stride = (size_t)a.nl * N / 4;  // uint4 per row i
   for (uint32_t i = 0; i < a.g.L; i++) {
-    // entries of row i at the quad, consumed by the pointwise stage
-    uint4 e[2];
-#pragma unroll
-    for (int f = 0; f < 2; f++)
-      e[f] = __ldg(reinterpret_cast<const uint4*>(a.E + ((((size_t)f * a.g.H + h) * a.g.L + i) * a.nl + lane) * N) +
-                   tid);
+    uint32_t* const Dc = D + (i & 1) * 2 * PS;
     // sigma_5(a) (the inverse transform's input and the kept t) and sigma_5(b)
-    uint32_t ta[2][4], tb[2][4];
+    uint32_t ta[8], tb[8];
 #pragma unroll
-    for (int f = 0; f < 2; f++)
-#pragma unroll
-      for (int m = 0; m < 4; m++) ta[f][m] = A[f * PS + src[m]], tb[f][m] = B[f * PS + src[m]];
-    // inverse stages 0-1 from registers
-#pragma unroll
-    for (int f = 0; f < 2; f++) {
-      const Tw4 w = load_tw4(a.T.iw2[f], tid);
-      uint4 v = make_uint4(ta[f][0], ta[f][1], ta[f][2], ta[f][3]);
-      gs(v.x, v.y, w.b0, w.b0q, pr[f]);
-      gs(v.z, v.w, w.b1, w.b1q, pr[f]);
-      gs(v.x, v.z, w.a, w.aq, pr[f]);
-      gs(v.y, v.w, w.a, w.aq, pr[f]);
-      *reinterpret_cast<uint4*>(D + f * PS + qb) = v;
+    for (int m = 0; m < 8; m++) {
+      const uint32_t sp = m & 1 ? src[m >> 1] >> 16 : src[m >> 1] & 0xFFFFu;
+      ta[m] = A[f * PS + sp], tb[m] = B[f * PS + sp];
     }
-    __syncthreads();
-    pass8<CT, 64, true>(D, 1, 1, a.T, (void*)nullptr);
-    pass8<CT, 8, true>(D, 1, 1, a.T, (void*)nullptr);
+    // inverse stages 0-1 from registers, two quads
+#pragma unroll
+    for (int h4 = 0; h4 < 2; h4++) {
+      const Tw4 w = load_tw4(a.T.iw2[f], 2 * t + h4);
+      uint4 v = make_uint4(ta[4 * h4], ta[4 * h4 + 1], ta[4 * h4 + 2], ta[4 * h4 + 3]);
+      gs(v.x, v.y, w.b0, w.b0q, p);
+      gs(v.z, v.w, w.b1, w.b1q, p);
+      gs(v.x, v.z, w.a, w.aq, p);
+      gs(v.y, v.w, w.a, w.aq, p);
+      *reinterpret_cast<uint4*>(Dc + f * PS + qb + 4 * h4) = v;
+    }
+    half_sync();
+    pass8<CT, 64, true, 1>(Dc, 1, 1, a.T, (void*)nullptr);
+    pass8<CT, 8, true, 1>(Dc, 1, 1, a.T, (void*)nullptr);
     {
-      // last inverse pass (unscaled: N^-1 sits in the CRT constants), swap,
-      // high digit, first forward pass; factor f, group g, words g + 256 k
-      const int f = tid >> 8, g = tid & 255;
-      const int base = (int)phys(g);
+      // last inverse pass (unscaled: N^-1 sits in the CRT constants), the
+      // other factor's values at the same positions, high digit, first
+      // forward pass; group g = t, words g + 256 k
+      const int base = (int)phys(t);
       constexpr int STR = Geo8<1>::STR;
       uint32_t v[8];
-      uint32_t* y = D + f * PS + base;
+      uint32_t* y = Dc + f * PS + base;
 #pragma unroll
       for (int k = 0; k < 8; k++) v[k] = y[k * STR];
-      inv8_bf(v, load_tw8(a.T.iw2[f], 1, 0), pr[f]);
+      inv8_bf(v, load_tw8(a.T.iw2[f], 1, 0), p);
 #pragma unroll
       for (int k = 0; k < 8; k++) y[k * STR] = v[k];
       __syncthreads();
-      const uint32_t* z = D + (1 - f) * PS + base;
+      const uint32_t* z = Dc + (1 - f) * PS + base;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const uint32_t o = z[k * STR];
         const int32_t hd = f == 0 ? high_digit(v[k], o, a.cp[0], a.cp[1]) : high_digit(o, v[k], a.cp[0], a.cp[1]);
-        v[k] = hd < 0 ? (uint32_t)(hd + (int32_t)pr[f]) : (uint32_t)hd;
+        v[k] = hd < 0 ? (uint32_t)(hd + (int32_t)p) : (uint32_t)hd;
       }
-      fwd8_bf(v, load_tw8(a.T.fw2[f], 1, 0), pr[f]);
+      fwd8_bf(v, load_tw8(a.T.fw2[f], 1, 0), p);
       uint32_t* w = A + f * PS + base;
 #pragma unroll
       for (int k = 0; k < 8; k++) w[k * STR] = v[k];
-      __syncthreads();
+      half_sync();
     }
-    pass8<CT, 8, false>(A, 1, 1, a.T, (void*)nullptr);
-    pass8<CT, 64, false>(A, 1, 1, a.T, (void*)nullptr);
-    // forward stages 9-10 and the pointwise stage at the quad
+    // entries of row i at the positions, consumed by the pointwise stage
+    // (loaded here: the two forward passes cover their latency)
+    const uint4 e0 = __ldg(Erow + i * erow_stride + 2 * t), e1 = __ldg(Erow + i * erow_stride + 2 * t + 1);
+    pass8<CT, 8, false, 1>(A, 1, 1, a.T, (void*)nullptr);
+    pass8<CT, 64, false, 1>(A, 1, 1, a.T, (void*)nullptr);
+    // forward stages 9-10 and the pointwise stage at the two quads
 #pragma unroll
-    for (int f = 0; f < 2; f++) {
-      const ChainPrime& cp = a.cp[f];
-      const uint32_t p = pr[f];
-      const Tw4 w = load_tw4(a.T.fw2[f], tid);
-      uint4 v = *reinterpret_cast<const uint4*>(A + f * PS + qb);
+    for (int h4 = 0; h4 < 2; h4++) {
+      const Tw4 w = load_tw4(a.T.fw2[f], 2 * t + h4);
+      uint4 v = *reinterpret_cast<const uint4*>(A + f * PS + qb + 4 * h4);
       ct(v.x, v.z, w.a, w.aq, p);
       ct(v.y, v.w, w.a, w.aq, p);
       ct(v.x, v.y, w.b0, w.b0q, p);
       ct(v.z, v.w, w.b1, w.b1q, p);
       const uint32_t n1s[4] = {red(red(v.x, 2 * p), p), red(red(v.y, 2 * p), p), red(red(v.z, 2 * p), p),
                                red(red(v.w, 2 * p), p)};
-      const uint32_t es[4] = {e[f].x, e[f].y, e[f].z, e[f].w};
+      const uint4 e = h4 ? e1 : e0;
+      const uint32_t es[4] = {e.x, e.y, e.z, e.w};
+      uint32_t kc[6][4];
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+        const uint4 c = KC[((j * 2 + f) * 2 + h4) * 256 + t];
+        kc[j][0] = c.x, kc[j][1] = c.y, kc[j][2] = c.z, kc[j][3] = c.w;
+      }
       uint32_t an[4], bn[4];
 #pragma unroll
       for (int m = 0; m < 4; m++) {
-        const uint32_t n1 = n1s[m], t = ta[f][m];
-        an[m] = mont_reduce((uint64_t)t * kc[f][0][m] + (uint64_t)n1 * kc[f][1][m] + (uint64_t)es[m] * kc[f][2][m], p,
+        const int j = 4 * h4 + m;
+        const uint32_t n1 = n1s[m], tt = ta[j];
+        an[m] = mont_reduce((uint64_t)tt * kc[0][m] + (uint64_t)n1 * kc[1][m] + (uint64_t)es[m] * kc[2][m], p,
                             cp.pinv);
-        bn[m] = mont_reduce(((uint64_t)tb[f][m] << 32) + (uint64_t)t * kc[f][3][m] + (uint64_t)n1 * kc[f][4][m] +
-                                (uint64_t)es[m] * kc[f][5][m],
+        bn[m] = mont_reduce(((uint64_t)tb[j] << 32) + (uint64_t)tt * kc[3][m] + (uint64_t)n1 * kc[4][m] +
+                                (uint64_t)es[m] * kc[5][m],
                             p, cp.pinv);
       }
-      *reinterpret_cast<uint4*>(A + f * PS + qb) = make_uint4(an[0], an[1], an[2], an[3]);
-      *reinterpret_cast<uint4*>(B + f * PS + qb) = make_uint4(bn[0], bn[1], bn[2], bn[3]);
+      *reinterpret_cast<uint4*>(A + f * PS + qb + 4 * h4) = make_uint4(an[0], an[1], an[2], an[3]);
+      *reinterpret_cast<uint4*>(B + f * PS + qb + 4 * h4) = make_uint4(bn[0], bn[1], bn[2], bn[3]);
     }
-    __syncthreads();
+    half_sync();
   }
   uint32_t* o = a.out + ((((size_t)q * a.g.H + h) * CTXT_PARTS + part) * 2) * 2 * N;
 #pragma unroll
-  for (int f = 0; f < 2; f++) {
-    reinterpret_cast<uint4*>(o + (size_t)f * N)[tid] = *reinterpret_cast<const uint4*>(A + f * PS + qb);
-    reinterpret_cast<uint4*>(o + 2 * (size_t)N + (size_t)f * N)[tid] = *reinterpret_cast<const uint4*>(B + f * PS + qb);
+  for (int h4 = 0; h4 < 2; h4++) {
+    reinterpret_cast<uint4*>(o + (size_t)f * N)[2 * t + h4] = *reinterpret_cast<const uint4*>(A + f * PS + qb + 4 * h4);
+    reinterpret_cast<uint4*>(o + 2 * (size_t)N + (size_t)f * N)[2 * t + h4] =
+        *reinterpret_cast<const uint4*>(B + f * PS + qb + 4 * h4);
   }
 }
 
