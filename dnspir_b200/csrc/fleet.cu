@@ -492,6 +492,7 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
   double best = 1e30;
   int best_i = -1;
   int rc = DNSPIR_OK;
+  std::vector<std::pair<double, int>> ranked;  // overlap-schedule time per shape that ran
   for (int i = 0; i < count && rc == DNSPIR_OK; i++) {
     const int qg = sh[i].nq / 4;
     const int pad = (nb + qg - 1) / qg * qg;
@@ -511,29 +512,37 @@ int dnspir_fleet_tune_pipeline(dnspir_fleet* f, uint32_t batch, double* ms_per_s
       }
     }
     if (ms_per_shape) ms_per_shape[i] = ms;
+    if (ms > 0) ranked.emplace_back(ms, i);
     if (ms > 0 && ms < best) {
       best = ms;
       best_i = i;
     }
   }
-  // schedule: the best shape again with each group's primary phase waiting for
-  // the previous group's secondary phase (1), or for its last chunk (2); keep
-  // whichever of the three is fastest
+  // schedule: the three best shapes again with each group's primary phase
+  // waiting for the previous group's secondary phase (1), or for its last
+  // chunk (2); keep the fastest shape and schedule (a shape whose small CTAs
+  // share SMs well with an overlapping secondary phase is not always the best
+  // one when the phases run one after the other)
   int serial = 0;
-  for (int sched = 1; sched <= 2 && rc == DNSPIR_OK && best_i >= 0; sched++) {
-    f->tuned[nb] = best_i;
-    f->tuned_serial[nb] = sched;
-    rc = dnspir_fleet_process_queries(f, ptrs.data(), lens.data(), (uint32_t)(nb * groups), r.as<uint8_t>(), RB,
-                                      nullptr, 1);
-    if (rc == DNSPIR_OK) {
-      std::lock_guard<std::mutex> lk(f->mu);
-      float t = 0;
-      if (cudaEventElapsedTime(&t, f->tev[6], f->tev[17]) == cudaSuccess && t / 2 < best) {
-        serial = sched;
-        best = t / 2;
-        if (ms_per_shape) ms_per_shape[best_i] = best;
+  std::sort(ranked.begin(), ranked.end());
+  for (size_t r0 = 0; r0 < ranked.size() && r0 < 3 && rc == DNSPIR_OK; r0++) {
+    const int i = ranked[r0].second;
+    for (int sched = 1; sched <= 2 && rc == DNSPIR_OK; sched++) {
+      f->tuned[nb] = i;
+      f->tuned_serial[nb] = sched;
+      rc = dnspir_fleet_process_queries(f, ptrs.data(), lens.data(), (uint32_t)(nb * groups), r.as<uint8_t>(), RB,
+                                        nullptr, 1);
+      if (rc == DNSPIR_OK) {
+        std::lock_guard<std::mutex> lk(f->mu);
+        float t = 0;
+        if (cudaEventElapsedTime(&t, f->tev[6], f->tev[17]) == cudaSuccess && t / 2 < best) {
+          serial = sched;
+          best = t / 2;
+          best_i = i;
+          if (ms_per_shape) ms_per_shape[i] = best;
+        }
+        cudaGetLastError();
       }
-      cudaGetLastError();
     }
   }
   // chain form: the best shape and schedule again with the two-block-cluster

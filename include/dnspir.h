@@ -164,10 +164,10 @@ int dnspir_fleet_scan(dnspir_fleet* fleet, const uint32_t* qnat, uint32_t nq, ui
  * replies; zero query bytes, two timed groups after one warm-up) instead of
  * the scan alone: the shape that maximises responses/s when the secondary
  * phase of one group overlaps the scan of the next.  ms_per_shape receives
- * milliseconds per group.  The schedule is tuned too: the best shape is timed
- * again with each group's primary phase waiting for the previous group's
- * secondary phase, and again waiting only until that phase starts its last
- * chunk; the fastest of the three schedules is kept for the group size, and
+ * milliseconds per group.  The schedule is tuned too: the three fastest shapes
+ * are timed again with each group's primary phase waiting for the previous
+ * group's secondary phase, and again waiting only until that phase starts its
+ * last chunk; the fastest shape and schedule are kept for the group size, and
  * then the two-block-cluster form of the secondary chains is tried at every
  * chunk size (kept when faster; dnspir_fleet_set_schedule's +4). */
 int dnspir_fleet_tune_pipeline(dnspir_fleet* fleet, uint32_t batch, double* ms_per_shape, int* chosen);
