@@ -22,6 +22,10 @@ After the plain run, on the same fleet:
     responses/s, p50/p99 per-query latency and the scan's effective GB/s
     (B x slab bytes / scan time) in the "batched" object.
 Then, with the 2^22 fleet released (unless --quick):
+  * "config1": 2^15 entries (4 half shards on 2 distinct), the reference
+    bench's 16 index pairs one query per launch sequence, through host
+    buffers and as one group; the CPU leg compares the replies with the
+    oracle's bytes (cpu_baseline.config1);
   * "config3" / "config4": 2^20 entries (64 full shards, all resident) on the
     CUDA-core and on the tensor engine, groups of 16, 64 and 256;
   * "served": the served mix for a few seconds at 5000 queries/s (below).
@@ -577,11 +581,99 @@ def batched_leg(dp, torch, dev, entries, engine, sizes, groups, check_every=8):
     return out
 
 
+def config1_leg(dp, torch, dev, rank):
+    """BASELINE config 1, the reference's own CPU-runnable bench (`bench
+    --db-entries 32768 --preprocessed-db-count 2`, pir_wrapper.rs:493-615):
+    4 half shards on 2 distinct, the 16 index pairs of pir_wrapper.rs:562
+    (secondary index j mod 4) answered one query per launch sequence (device
+    events) and through host buffers, then as one group of 16.  Every reply
+    decrypts; the replies and the shards' coefficients are kept for the CPU
+    leg, which compares them with the oracle's bytes."""
+    entries = 1 << 15
+    l1, l2, shards = dp.get_database_shape(entries)
+    per = 8 * l1
+    fleet = dp.Fleet(entries, 2)
+    fleet.set_engine(dp.ENGINE_TENSOR)
+    co = torch.empty((2, per, dp.N), dtype=torch.uint16, device=dev)
+    for i in range(2):
+        dp.pack_payloads(shard_payload(torch, i, per, dev, seed0=5000), co[i], device=dev.index or 0)
+    fleet.set_shards(0, co)
+    pairs = [(i, j % shards) for i, j in REFERENCE_INDICES]
+    qs = [dp.prepare_query(hashlib.sha256(f"c1-{rank}-{k}".encode()).digest(), i, j, l1, l2)
+          for k, (i, j) in enumerate(pairs)]
+    qlen = len(qs[0][0])
+    qdev = torch.tensor(np.frombuffer(b"".join(q for q, _ in qs), dtype=np.uint8).reshape(len(qs), qlen), device=dev)
+    rdev = torch.zeros((len(qs), dp.reply_bytes()), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    fleet.set_stream(stream.cuda_stream)
+    for _ in range(3):  # warm-up
+        fleet.process_queries_device(qdev[:2], rdev[:2])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fleet.process_queries_device(qdev, rdev)  # one query per launch sequence, back to back
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    lat = fleet.batch_timings(len(qs))[0]
+    fleet.set_batch(16)
+    rb = torch.zeros_like(rdev)
+    fleet.process_queries_device(qdev, rb)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fleet.process_queries_device(qdev, rb)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    group_ms = e0.elapsed_time(e1)
+    fleet.set_batch(1)
+    fleet.set_stream(None)
+    t0 = time.perf_counter()
+    host = fleet.process_queries([q for q, _ in qs])
+    e2e_s = time.perf_counter() - t0
+    dev_replies = [r.tobytes() for r in rdev.cpu().numpy()]
+    grp_replies = [r.tobytes() for r in rb.cpu().numpy()]
+    coeffs = co.cpu().numpy()
+    ok = sum(int(np.array_equal(dp.process_reply(r, sk), coeffs[j % 2][i]) and r == h and r == g)
+             for (i, j), (q, sk), r, h, g in zip(pairs, qs, dev_replies, host, grp_replies))
+    fleet.close()
+    del co, qdev, rdev, rb
+    out = {"entries": entries, "shards": shards, "distinct": 2, "primary_order": l1, "secondary_order": l2,
+           "query_bytes": qlen, "indices": "pir_wrapper.rs:562, secondary index j mod 4",
+           "responses_per_sec": len(qs) / (plain_ms * 1e-3), "p50_ms": float(np.median(lat)),
+           "e2e_responses_per_sec": len(qs) / e2e_s, "group16_responses_per_sec": len(qs) / (group_ms * 1e-3),
+           "checked": {"decrypted_ok": ok, "of": len(qs), "note": "device, host and group replies equal, and decrypt"}}
+    return out, {"coeffs": coeffs, "queries": [q for q, _ in qs], "replies": dev_replies, "shards": shards}
+
+
+def config1_cpu(check):
+    """The oracle (C++ restatement of process_query) on config 1's shards and
+    queries: its replies against the GPU's, byte for byte, and its time."""
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    orc.set_num_threads(threads)
+    refs = []
+    for i in range(2):
+        d = orc.Database(11, check["coeffs"].shape[1] // 8)
+        d.set_db(check["coeffs"][i])
+        refs.append(d)
+    fleet_refs = [refs[k % 2] for k in range(check["shards"])]
+    t0 = time.perf_counter()
+    want = [orc.process_query(fleet_refs, q) for q in check["queries"]]
+    dt = time.perf_counter() - t0
+    same = sum(int(a == b) for a, b in zip(want, check["replies"]))
+    return {"value": len(want) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "the oracle's process_query (scalar C++ restatement) on the 16 queries of config 1",
+            "gpu_replies_equal_oracle": {"equal": same, "of": len(want)}}
+
+
 def extra_legs(args, dp, torch, dev, local_rank):
-    """BASELINE configs 3, 4 (2^20, both engines) and 5 (served mix), run
-    after the 2^22 fleet is released."""
+    """BASELINE configs 1 (2^15), 3, 4 (2^20, both engines) and 5 (served
+    mix), run after the 2^22 fleet is released."""
     legs = {}
     try:
+        legs["config1"], legs["_config1_check"] = config1_leg(dp, torch, dev, 0)
+        if legs["config1"]["checked"]["decrypted_ok"] != legs["config1"]["checked"]["of"]:
+            raise RuntimeError("config 1: a reply failed its check")
         legs["config3"] = batched_leg(dp, torch, dev, 1 << 20, "cuda", [16, 64, 256], 2)
         legs["config3"]["note"] = ("CUDA-core modular-MAC scan (u32 x u32 -> u64), one launch per group; the reference "
                                    "rule gives full shards at 2^20 (pir_wrapper.rs:188, 223-227)")
@@ -849,9 +941,16 @@ def main():
         "clocks": clk,
         "checked": {"decrypted_ok": ok, "of": args.steps},
     }
+    check1 = legs.pop("_config1_check", None)
     line.update(legs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_line(args, l1, l2, shards)
+        if check1 is not None:
+            c1 = config1_cpu(check1)
+            line["cpu_baseline"]["config1"] = c1
+            if c1["gpu_replies_equal_oracle"]["equal"] != c1["gpu_replies_equal_oracle"]["of"]:
+                print(json.dumps({"error": "config 1: GPU replies differ from the oracle's"}), flush=True)
+                return 1
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:
