@@ -424,8 +424,10 @@ def cpu_sample_text(l1, l2, shards, distinct, steps, used, scan_s, sec_s):
     return (f"{steps} whole queries timed for real: main_pir_loop restatement (AVX-512 op sequence, "
             f"{'AVX-512 present' if orc.cpu_has_avx512() else 'NO AVX-512: scalar loop'}) over all {shards} shards "
             f"({min(distinct, shards)} distinct slabs in host RAM, shard k -> k mod {min(distinct, shards)}) on {used} "
-            f"threads, {scan_s:.2f} s per query, then the scalar oracle's secondary phase (set_db + scan at order "
-            f"{l2}, parallel over the 16 (half, lane) chains), {sec_s:.2f} s per query")
+            f"threads, {scan_s:.2f} s per query, then the secondary phase (set_db + scan at order {l2}) on "
+            + ("the AVX-512 restatement (8 lanes per register as simd_zn.rs; each half's chain on 4 threads split "
+               "as partial_gal's join / par_iter)" if orc.cpu_has_avx512() else "the scalar oracle")
+            + f", {sec_s:.2f} s per query")
 
 
 def run_reference(args, rank):

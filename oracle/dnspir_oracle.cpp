@@ -37,6 +37,7 @@
 #include <vector>
 #include <atomic>
 #include <thread>
+#include <immintrin.h>
 
 typedef unsigned __int128 u128;
 typedef __int128 i128;
@@ -1125,6 +1126,456 @@ static void get_database_shape(size_t num_entries, IndexGroup* ig1, IndexGroup* 
 // ====================================================================== C ABI
 using namespace orc;
 
+// ===================================================== vectorised restatement
+// The same set_transformed_entries, preprocess (partial_gal chain) and
+// perform_pir_split as above, on the reference's vector shape: the 8 SIMD
+// lanes of a slot in one AVX-512 register of 8 x u64 (simd_zn.rs
+// SpecialZnx8, avx.rs), products by _mm512_mul_epu32 and the reduction for
+// p = 2^K - alpha of simd_zn.rs:197-230 (two shift-multiply-subtract steps,
+// then one conditional subtraction, so every value is canonical as in the
+// scalar code), the chain of each half run for all 8 lanes at once and the
+// halves in parallel (the reference's parallelism).  Used to time the
+// secondary phase of the CPU arm; tests check it equals the scalar code
+// array for array.  Compiled for AVX-512 in these functions only; callers
+// check orc_cpu_has_avx512 first.
+#define ORC_AVX512 __attribute__((target("avx512f,avx512dq")))
+
+namespace vec {
+
+// 64-byte aligned array of n vectors (std::vector drops __m512i's alignment)
+struct VBuf {
+  __m512i* p;
+  explicit VBuf(size_t n) : p(static_cast<__m512i*>(aligned_alloc(64, (n ? n : 1) * sizeof(__m512i)))) {
+    if (!p) throw std::runtime_error("out of host memory");
+  }
+  ~VBuf() { free(p); }
+  VBuf(const VBuf&) = delete;
+  VBuf& operator=(const VBuf&) = delete;
+  __m512i& operator[](size_t i) { return p[i]; }
+  __m512i* data() { return p; }
+};
+
+template <int PI>
+struct Pr {
+  static constexpr uint64_t P = PI ? Q2 : Q1;
+  static constexpr int K = PI ? 25 : 26;
+};
+
+// a * b mod p for a, b < p (canonical out)
+template <int PI>
+ORC_AVX512 static inline __m512i mulmod(__m512i a, __m512i b) {
+  const __m512i p = _mm512_set1_epi64((long long)Pr<PI>::P);
+  __m512i x = _mm512_mul_epu32(a, b);
+  x = _mm512_sub_epi64(x, _mm512_mul_epu32(_mm512_srli_epi64(x, Pr<PI>::K), p));
+  x = _mm512_sub_epi64(x, _mm512_mul_epu32(_mm512_srli_epi64(x, Pr<PI>::K), p));
+  return _mm512_min_epu64(x, _mm512_sub_epi64(x, p));
+}
+template <int PI>
+ORC_AVX512 static inline __m512i addmod(__m512i a, __m512i b) {
+  const __m512i p = _mm512_set1_epi64((long long)Pr<PI>::P);
+  const __m512i s = _mm512_add_epi64(a, b);
+  return _mm512_min_epu64(s, _mm512_sub_epi64(s, p));
+}
+template <int PI>
+ORC_AVX512 static inline __m512i submod(__m512i a, __m512i b) {
+  const __m512i p = _mm512_set1_epi64((long long)Pr<PI>::P);
+  const __m512i d = _mm512_sub_epi64(_mm512_add_epi64(a, p), b);
+  return _mm512_min_epu64(d, _mm512_sub_epi64(d, p));
+}
+
+// Dft::apply on n vectors (the same radix-2 DIT with bit reversal)
+template <int PI>
+ORC_AVX512 static void dft8(const Dft& d, __m512i* x) {
+  const size_t n = d.n;
+  for (size_t i = 0; i < n; i++) {
+    const size_t r = d.rev[i];
+    if (r > i) std::swap(x[i], x[r]);
+  }
+  for (size_t h = 1; h < n; h <<= 1)
+    for (size_t j = 0; j < h; j++) {
+      const __m512i w = _mm512_set1_epi64((long long)d.tw[h + j]);
+      for (size_t i = 0; i < n; i += 2 * h) {
+        const __m512i u = x[i + j], v = mulmod<PI>(x[i + j + h], w);
+        x[i + j] = addmod<PI>(u, v);
+        x[i + j + h] = submod<PI>(u, v);
+      }
+    }
+}
+template <int PI>
+ORC_AVX512 static void weighted_ntt8(const Ring& R, __m512i* x) {
+  for (size_t i = 0; i < R.n; i++) x[i] = mulmod<PI>(x[i], _mm512_set1_epi64((long long)R.zneg[PI][i]));
+  dft8<PI>(R.fwd[PI], x);
+}
+template <int PI>
+ORC_AVX512 static void inv_weighted_ntt8(const Ring& R, __m512i* x) {
+  dft8<PI>(R.inv[PI], x);
+  for (size_t i = 0; i < R.n; i++) {
+    const uint64_t s = R.md[PI].mul(R.ninv[PI], R.zpos[PI][i]);
+    x[i] = mulmod<PI>(x[i], _mm512_set1_epi64((long long)s));
+  }
+}
+
+ORC_AVX512 static inline __m512i ld(const uint64_t* p) { return _mm512_loadu_si512((const void*)p); }
+ORC_AVX512 static inline void st(uint64_t* p, __m512i v) { _mm512_storeu_si512((void*)p, v); }
+
+// STEP 2 of set_transformed_entries for column j
+ORC_AVX512 static void col_ntt(const Ring& R, uint64_t* M, size_t l, size_t j) {
+  const size_t N = R.n;
+  VBuf c(N);
+  for (size_t i = 0; i < N; i++) c[i] = ld(&M[(i * l + j) * SIMD]);
+  weighted_ntt8<0>(R, c.data());
+  for (size_t i = 0; i < N; i++) st(&M[(i * l + j) * SIMD], c[i]);
+}
+// coset_ntt of row i (the scalar function's steps on vectors)
+ORC_AVX512 static void row_coset_ntt(const Ring& R, const IndexGroup& ig, int64_t zeta_power, uint64_t* values,
+                                     const Dft& fft_l) {
+  const size_t N = ig.N, l = ig.l;
+  const int64_t m = 2 * (int64_t)N;
+  const Mod& md = R.md[0];
+  const int64_t zp = mod_floor(zeta_power, m);
+  const int64_t coset = zp % (m / (int64_t)l);
+  const uint64_t z = powmod(R.zeta[0], (uint64_t)coset, R.p[0]);
+  const uint64_t zinv = invmod(z, R.p[0]);
+  VBuf v(l), old(l);
+  uint64_t cur = 1;
+  for (size_t i = 0; i < l; i++) {
+    v[i] = mulmod<0>(ld(&values[i * SIMD]), _mm512_set1_epi64((long long)cur));
+    cur = md.mul(cur, zinv);
+  }
+  dft8<0>(fft_l, v.data());
+  auto g2i = [&](int64_t x) -> size_t { return (size_t)((mod_floor(-x, m) - coset) / (m / (int64_t)l)); };
+  const int64_t zpn = mod_floor(-zp, m);
+  memcpy(old.data(), v.data(), l * sizeof(__m512i));
+  int64_t gpow = 1;
+  for (size_t i = 0; i < l; i++) {
+    size_t src;
+    if (ig.conj()) {
+      if (i == N / 2) gpow = 1;
+      src = i < N / 2 ? g2i(zpn * gpow % m) : g2i(zp * gpow % m);
+    } else {
+      src = g2i(zpn * gpow % m);
+    }
+    gpow = gpow * 5 % m;
+    st(&values[i * SIMD], old[src]);
+  }
+}
+// STEP 6 for column col: iNTT, lift, * l^-1 mod t, centred lift, NTT in q1 and q2
+ORC_AVX512 static void col_lift(const Ring& R, Shard& db, const uint64_t* M, size_t l, size_t col, int64_t scale) {
+  const size_t N = R.n, L = db.ig.loop_len();
+  VBuf c(N), r0(N), r1(N);
+  for (size_t i = 0; i < N; i++) c[i] = ld(&M[(i * l + col) * SIMD]);
+  inv_weighted_ntt8<0>(R, c.data());
+  alignas(64) uint64_t cv[SIMD], a0[SIMD], a1[SIMD];
+  for (size_t i = 0; i < N; i++) {
+    _mm512_store_si512((void*)cv, c[i]);
+    for (int k = 0; k < SIMD; k++) {
+      const int64_t vv = smallest_lift((int64_t)cv[k], Q1);
+      const int64_t w = smallest_lift(mod_floor(mod_floor(vv, TPLAIN) * scale, TPLAIN), TPLAIN);
+      a0[k] = (uint64_t)mod_floor(w, Q1);
+      a1[k] = (uint64_t)mod_floor(w, Q2);
+    }
+    r0[i] = _mm512_load_si512((const void*)a0);
+    r1[i] = _mm512_load_si512((const void*)a1);
+  }
+  weighted_ntt8<0>(R, r0.data());
+  weighted_ntt8<1>(R, r1.data());
+  const int half = col < L ? 0 : 1;
+  const size_t row = col < L ? col : col - L;
+  for (size_t i = 0; i < N; i++) {
+    st(&db.te[half][0][(row * N + i) * SIMD], r0[i]);
+    st(&db.te[half][1][(row * N + i) * SIMD], r1[i]);
+  }
+}
+
+}  // namespace vec
+
+// set_transformed_entries on vectors: STEP 1, 4 and 5 move data as the scalar
+// code does; STEP 2, 3 and 6 are the vector transforms above
+static void set_transformed_entries_vec(Shard& db, const uint16_t* entries) {
+  const Ring& R = *db.R;
+  const size_t N = R.n, l = db.ig.l, L = db.ig.loop_len();
+  const int64_t m = 2 * (int64_t)N;
+  ORC_CHECK(2 * TPLAIN * (int64_t)N < Q1, "max_coeff >= q1");
+  std::vector<uint64_t> M(N * l * SIMD);
+  parallel_for(l, [&](size_t j) {
+    for (int k = 0; k < SIMD; k++) {
+      const uint16_t* e = entries + ((size_t)j * SIMD + k) * N;
+      for (size_t i = 0; i < N; i++) M[(i * l + j) * SIMD + k] = e[i];
+    }
+  });
+  parallel_for(l, [&](size_t j) { vec::col_ntt(R, M.data(), l, j); });
+  {
+    size_t logl = 0;
+    while (((size_t)1 << logl) < l) logl++;
+    uint64_t omega = powmod(R.zeta[0], (uint64_t)(m / (int64_t)l), R.p[0]);
+    Dft fft_l(R.p[0], l, invmod(omega, R.p[0]));
+    int64_t base_power = mod_floor(-(int64_t)db.ig.qbp(), m);
+    parallel_for(N, [&](size_t i) {
+      vec::row_coset_ntt(R, db.ig, mod_floor(idx2gal(N, (int64_t)i) * base_power, m), &M[i * l * SIMD], fft_l);
+    });
+  }
+  {
+    int64_t g_inv = (int64_t)invmod(5, (uint64_t)m);
+    parallel_for(l, [&](size_t j) {
+      int64_t aut = (int64_t)powmod((uint64_t)g_inv, j, (uint64_t)m);
+      std::vector<uint64_t> c(N * SIMD);
+      for (size_t i = 0; i < N; i++) {
+        size_t src = gal2idx(N, aut * idx2gal(N, (int64_t)i) % m);
+        memcpy(&c[i * SIMD], &M[(src * l + j) * SIMD], SIMD * 8);
+      }
+      for (size_t i = 0; i < N; i++) memcpy(&M[(i * l + j) * SIMD], &c[i * SIMD], SIMD * 8);
+    });
+  }
+  parallel_for(N, [&](size_t i) {
+    uint64_t* row = &M[i * l * SIMD];
+    auto rev = [&](size_t a, size_t b) {
+      while (b > a + 1) {
+        b--;
+        for (int k = 0; k < SIMD; k++) std::swap(row[a * SIMD + k], row[b * SIMD + k]);
+        a++;
+      }
+    };
+    if (db.ig.conj()) {
+      rev(0, N / 2);
+      rev(N / 2, N);
+    } else {
+      rev(0, l);
+    }
+  });
+  for (int c = 0; c < 2; c++)
+    for (int pi = 0; pi < 2; pi++) db.te[c][pi].assign(db.ig.conj() || c == 0 ? L * N * SIMD : 0, 0);
+  const int64_t scale = (int64_t)invmod((uint64_t)(l % TPLAIN), (uint64_t)TPLAIN);
+  parallel_for(l, [&](size_t col) { vec::col_lift(R, db, M.data(), l, col, scale); });
+  db.has_reply_a = false;
+}
+
+namespace vec {
+
+// Spin barrier for the few threads that share one half's chain step.
+struct TeamBarrier {
+  std::atomic<int> count{0};
+  std::atomic<int> gen{0};
+  int n;
+  explicit TeamBarrier(int n_) : n(n_) {}
+  void wait() {
+    const int g = gen.load(std::memory_order_acquire);
+    if (count.fetch_add(1, std::memory_order_acq_rel) == n - 1) {
+      count.store(0, std::memory_order_relaxed);
+      gen.store(g + 1, std::memory_order_release);
+    } else {
+      while (gen.load(std::memory_order_acquire) == g) _mm_pause();
+    }
+  }
+};
+
+// One step of the chain of half c, thread t of 4, as the reference splits it
+// (base_pir.rs:496-594): the two factors' inverse transforms side by side
+// (join), the decomposition split over positions (par_iter), the four digit
+// transforms side by side (par_iter over digits x join over factors), then the
+// pointwise reply_a and the next sum, split over positions.
+struct ChainTeam {
+  Shard* db;
+  int c;
+  size_t N;
+  std::vector<size_t> gmap;
+  VBuf buf;
+  __m512i *sum[2], *ra[2], *dig[2][2], *gal[2], *gk[2][2], *qa[2];
+  TeamBarrier bar{4};
+  ChainTeam(Shard* db_, int c_, size_t N_) : db(db_), c(c_), N(N_), gmap(N_), buf(16 * N_) {
+    for (int pi = 0; pi < 2; pi++) {
+      sum[pi] = &buf[(0 + pi) * N];
+      ra[pi] = &buf[(2 + pi) * N];
+      dig[0][pi] = &buf[(4 + pi) * N];
+      dig[1][pi] = &buf[(6 + pi) * N];
+      gal[pi] = &buf[(8 + pi) * N];
+      gk[0][pi] = &buf[(10 + pi) * N];
+      gk[1][pi] = &buf[(12 + pi) * N];
+      qa[pi] = &buf[(14 + pi) * N];
+    }
+  }
+};
+
+ORC_AVX512 static void chain_thread(ChainTeam& T, int t) {
+  Shard& db = *T.db;
+  const Ring& R = *db.R;
+  const size_t N = T.N, L = db.ig.loop_len();
+  const size_t j0 = N * t / 4, j1 = N * (t + 1) / 4;
+  const __m512i q2inv1 = _mm512_set1_epi64((long long)invmod(Q2 % Q1, Q1));
+  const __m512i q1inv2 = _mm512_set1_epi64((long long)invmod(Q1 % Q2, Q2));
+  const __m512i vq1 = _mm512_set1_epi64(Q1), vq2 = _mm512_set1_epi64(Q2), vqq = _mm512_set1_epi64(QQ);
+  const __m512i vqq2 = _mm512_set1_epi64(QQ / 2), half = _mm512_set1_epi64((long long)1 << (LOG2_B - 1));
+  const __m512i zero = _mm512_setzero_si512();
+  for (size_t i = 0; i < L; i++) {
+    // gal(sum) and its inverse transform, one factor per thread (base_pir.rs:509-519)
+    if (t < 2) {
+      for (size_t j = 0; j < N; j++) T.gal[t][T.gmap[j]] = T.sum[t][j];
+      if (t == 0)
+        inv_weighted_ntt8<0>(R, T.gal[0]);
+      else
+        inv_weighted_ntt8<1>(R, T.gal[1]);
+    }
+    T.bar.wait();
+    // centred CRT lift and the two digits (base_pir.rs:541-571)
+    for (size_t j = j0; j < j1; j++) {
+      const __m512i x1 = mulmod<0>(T.gal[0][j], q2inv1);
+      const __m512i x2 = mulmod<1>(T.gal[1][j], q1inv2);
+      __m512i v = _mm512_add_epi64(_mm512_mul_epu32(x1, vq2), _mm512_mul_epu32(x2, vq1));
+      v = _mm512_mask_sub_epi64(v, _mm512_cmpgt_epi64_mask(v, vqq), v, vqq);
+      v = _mm512_mask_sub_epi64(v, _mm512_cmpgt_epi64_mask(v, vqq2), v, vqq);
+      __m512i cur_v = v;
+      for (int d = 0; d < 2; d++) {
+        const __m512i high = _mm512_srai_epi64(_mm512_add_epi64(cur_v, half), LOG2_B);
+        const __m512i low = _mm512_sub_epi64(cur_v, _mm512_slli_epi64(high, LOG2_B));
+        T.dig[d][0][j] = _mm512_mask_add_epi64(low, _mm512_cmplt_epi64_mask(low, zero), low, vq1);
+        __m512i r = _mm512_mask_add_epi64(low, _mm512_cmplt_epi64_mask(low, zero), low, vq2);
+        r = _mm512_mask_add_epi64(r, _mm512_cmplt_epi64_mask(r, zero), r, vq2);
+        r = _mm512_mask_sub_epi64(r, _mm512_cmpge_epi64_mask(r, vq2), r, vq2);
+        T.dig[d][1][j] = r;
+        cur_v = high;
+      }
+    }
+    T.bar.wait();
+    // the four digit transforms, one per thread (base_pir.rs:574-579)
+    if (t % 2 == 0)
+      weighted_ntt8<0>(R, T.dig[t / 2][0]);
+    else
+      weighted_ntt8<1>(R, T.dig[t / 2][1]);
+    T.bar.wait();
+    // reply_a, the stored digits and the next sum (preprocess_loop)
+    for (size_t j = j0; j < j1; j++) {
+      const __m512i r0 = addmod<0>(mulmod<0>(T.dig[0][0][j], T.gk[0][0][j]), mulmod<0>(T.dig[1][0][j], T.gk[1][0][j]));
+      const __m512i r1 = addmod<1>(mulmod<1>(T.dig[0][1][j], T.gk[0][1][j]), mulmod<1>(T.dig[1][1][j], T.gk[1][1][j]));
+      for (int d = 0; d < 2; d++)
+        for (int pi = 0; pi < 2; pi++) st(&db.gk[T.c][d][pi][(i * N + j) * SIMD], T.dig[d][pi][j]);
+      T.sum[0][j] = addmod<0>(r0, mulmod<0>(T.qa[0][j], ld(&db.te[T.c][0][(i * N + j) * SIMD])));
+      T.sum[1][j] = addmod<1>(r1, mulmod<1>(T.qa[1][j], ld(&db.te[T.c][1][(i * N + j) * SIMD])));
+    }
+    T.bar.wait();
+  }
+}
+
+// the chain of half c for all 8 lanes (preprocess_loop, base_pir.rs:782-863)
+ORC_AVX512 static void chain_half(Shard& db, int c, const std::vector<uint64_t> gka[2][2],
+                                  const std::vector<uint64_t> qa[2], std::vector<uint64_t> sums_out[2]) {
+  const Ring& R = *db.R;
+  const size_t N = R.n;
+  const int64_t m = 2 * (int64_t)N;
+  const int64_t inv_g = (int64_t)invmod(5, (uint64_t)m);
+  ChainTeam T(&db, c, N);
+  for (size_t i = 0; i < N; i++) T.gmap[i] = gal2idx(N, inv_g * idx2gal(N, (int64_t)i) % m);
+  for (size_t j = 0; j < N; j++)
+    for (int pi = 0; pi < 2; pi++) {
+      T.sum[pi][j] = _mm512_setzero_si512();
+      for (int d = 0; d < 2; d++) T.gk[d][pi][j] = ld(&gka[d][pi][j * SIMD]);
+      T.qa[pi][j] = ld(&qa[pi][j * SIMD]);
+    }
+  std::vector<std::thread> th;
+  for (int t = 1; t < 4; t++) th.emplace_back([&T, t]() { chain_thread(T, t); });
+  chain_thread(T, 0);
+  for (auto& x : th) x.join();
+  for (int pi = 0; pi < 2; pi++) sums_out[pi].assign(N * SIMD, 0);
+  for (size_t j = 0; j < N; j++) {
+    st(&sums_out[0][j * SIMD], T.sum[0][j]);
+    st(&sums_out[1][j * SIMD], T.sum[1][j]);
+  }
+}
+
+// main_pir_loop on vectors (same recurrence, reduction every reduce_every rows)
+ORC_AVX512 static void main_pir_loop8(size_t N, size_t len, size_t reduce_every, const Mod& md,
+                                      std::vector<uint64_t>& sum, const std::vector<size_t>& gal,
+                                      const uint64_t* qry_b, const uint64_t* gk0, const uint64_t* gk1,
+                                      const uint64_t* ipg0, const uint64_t* ipg1, const uint64_t* te) {
+  std::vector<uint64_t> sum_new(N * SIMD, 0);
+  size_t index = 0;
+  for (size_t io = 0; io < len; io += reduce_every) {
+    const size_t cnt = std::min(len - io, reduce_every);
+    for (size_t ii = 0; ii < cnt; ii++) {
+      for (size_t j = 0; j < N; j++) {
+        const size_t e = (index + j) * SIMD;
+        __m512i acc = ld(&sum[j * SIMD]);
+        acc = _mm512_add_epi64(acc, _mm512_mul_epu32(ld(&ipg0[e]), ld(&gk0[j * SIMD])));
+        acc = _mm512_add_epi64(acc, _mm512_mul_epu32(ld(&ipg1[e]), ld(&gk1[j * SIMD])));
+        acc = _mm512_add_epi64(acc, _mm512_mul_epu32(ld(&te[e]), ld(&qry_b[j * SIMD])));
+        st(&sum_new[gal[j] * SIMD], acc);
+      }
+      index += N;
+      std::swap(sum, sum_new);
+    }
+    for (size_t j = 0; j < N * SIMD; j++) sum[j] = md.red(sum[j]);
+  }
+}
+
+}  // namespace vec
+
+static void preprocess_vec(Shard& db) {
+  const Ring& R = *db.R;
+  const size_t N = R.n, L = db.ig.loop_len();
+  std::vector<uint64_t> gka[2][2];
+  for (int d = 0; d < 2; d++) to_simd_element_same(R, gk_a(N, d), gka[d]);
+  std::vector<uint64_t> qa[2][2];
+  for (int c = 0; c < (db.ig.conj() ? 2 : 1); c++) to_simd_element_same(R, qry_a(N, db.used_seeds, c), qa[c]);
+  for (int c = 0; c < 2; c++)
+    for (int d = 0; d < 2; d++)
+      for (int pi = 0; pi < 2; pi++) db.gk[c][d][pi].assign(db.ig.conj() || c == 0 ? L * N * SIMD : 0, 0);
+  const int halves = db.ig.conj() ? 2 : 1;
+  std::vector<uint64_t> sums[2][2];
+  parallel_for((size_t)halves, [&](size_t c) { vec::chain_half(db, (int)c, gka, qa[c], sums[c]); });
+  for (int pi = 0; pi < 2; pi++) {
+    db.reply_a[pi].assign(N * SIMD, 0);
+    for (size_t j = 0; j < N * SIMD; j++)
+      db.reply_a[pi][j] = halves == 2 ? R.md[pi].add(sums[0][pi][j], sums[1][pi][j]) : sums[0][pi][j];
+  }
+  db.has_reply_a = true;
+}
+
+// perform_pir_split with the vector scan (everything else as the scalar function)
+static void perform_pir_split_vec(const Shard& db, const QueryRef q[SIMD], Poly out[SIMD]) {
+  const Ring& R = *db.R;
+  const size_t N = R.n, L = db.ig.loop_len();
+  const int64_t m = 2 * (int64_t)N;
+  std::vector<uint64_t> qb[2], qcb[2], gkb[2][2];
+  {
+    const Poly* els[SIMD];
+    for (int k = 0; k < SIMD; k++) els[k] = q[k].qry_b;
+    to_simd_element(R, els, qb);
+    if (db.ig.conj()) {
+      for (int k = 0; k < SIMD; k++) {
+        ORC_CHECK(q[k].qry_conj_b, "conjugate query must be given when index subgroup requires conjugation");
+        els[k] = q[k].qry_conj_b;
+      }
+      to_simd_element(R, els, qcb);
+    }
+    for (int d = 0; d < 2; d++) {
+      for (int k = 0; k < SIMD; k++) els[k] = q[k].gk_b[d];
+      to_simd_element(R, els, gkb[d]);
+    }
+  }
+  const int64_t inv_g = (int64_t)invmod(5, (uint64_t)m);
+  std::vector<size_t> gal(N);
+  for (size_t i = 0; i < N; i++) gal[i] = (size_t)((mod_floor(inv_g * (2 * (int64_t)i + 1), m) - 1) / 2);
+  std::vector<uint64_t> sum[2], sum_conj[2];
+  const int halves = db.ig.conj() ? 2 : 1;
+  u128 rb0 = 2 * (u128)R.p[0], rb1 = 2 * (u128)R.p[1];
+  const size_t reduce_every = (size_t)std::min((u128)UINT64_MAX / rb0 / rb0 / (GK_DIGITS + 1),
+                                               (u128)UINT64_MAX / rb1 / rb1 / (GK_DIGITS + 1));
+  parallel_for((size_t)2 * halves, [&](size_t u) {
+    const int pi = (int)(u % 2), c = (int)(u / 2);
+    std::vector<uint64_t>& s = c ? sum_conj[pi] : sum[pi];
+    s.assign(N * SIMD, 0);
+    vec::main_pir_loop8(N, L, reduce_every, R.md[pi], s, gal, (c ? qcb : qb)[pi].data(), gkb[0][pi].data(),
+                        gkb[1][pi].data(), db.gk[c][0][pi].data(), db.gk[c][1][pi].data(), db.te[c][pi].data());
+  });
+  for (int pi = 0; pi < 2; pi++) {
+    if (halves == 2)
+      for (size_t j = 0; j < N * SIMD; j++) sum[pi][j] += sum_conj[pi][j];
+    std::vector<uint64_t> pm(N * SIMD);
+    for (size_t i = 0; i < N; i++)
+      for (int k = 0; k < SIMD; k++) pm[i * SIMD + k] = R.md[pi].red(sum[pi][gal[i] * SIMD + k]);
+    sum[pi].swap(pm);
+  }
+  from_simd_element(R, sum, out);
+}
+
 struct orc_db {
   Shard s;
 };
@@ -1221,6 +1672,15 @@ int orc_db_set_db(orc_db* d, const uint16_t* entries) {
     preprocess(d->s);
   })
 }
+// the vectorised restatement (AVX-512; the caller checks orc_cpu_has_avx512)
+int orc_db_set_db_vec(orc_db* d, const uint16_t* entries) {
+  ORC_TRY({
+    for (size_t i = 0; i < (size_t)SIMD * d->s.ig.l * d->s.R->n; i++)
+      ORC_CHECK(entries[i] < TPLAIN, "entry coefficient must be below t");
+    set_transformed_entries_vec(d->s, entries);
+    preprocess_vec(d->s);
+  })
+}
 int orc_db_set_transformed_entries(orc_db* d, const uint16_t* entries) {
   ORC_TRY({ set_transformed_entries(d->s, entries); })
 }
@@ -1264,6 +1724,25 @@ int orc_db_perform_pir_split(orc_db* d, const int64_t* qry_b, const int64_t* qry
     }
     Poly o[SIMD];
     perform_pir_split(d->s, qr, o);
+    for (int k = 0; k < SIMD; k++) memcpy(out + k * N, o[k].data(), N * 8);
+  })
+}
+
+int orc_db_perform_pir_split_vec(orc_db* d, const int64_t* qry_b, const int64_t* qry_conj_b, const int64_t* gk_b,
+                                 int64_t* out) {
+  ORC_TRY({
+    size_t N = d->s.R->n;
+    std::vector<Poly> qb(SIMD), qcb(SIMD), g0(SIMD), g1(SIMD);
+    QueryRef qr[SIMD];
+    for (int k = 0; k < SIMD; k++) {
+      qb[k].assign(qry_b + k * N, qry_b + (k + 1) * N);
+      if (qry_conj_b) qcb[k].assign(qry_conj_b + k * N, qry_conj_b + (k + 1) * N);
+      g0[k].assign(gk_b + (2 * k) * N, gk_b + (2 * k + 1) * N);
+      g1[k].assign(gk_b + (2 * k + 1) * N, gk_b + (2 * k + 2) * N);
+      qr[k] = QueryRef{&qb[k], qry_conj_b ? &qcb[k] : nullptr, {&g0[k], &g1[k]}};
+    }
+    Poly o[SIMD];
+    perform_pir_split_vec(d->s, qr, o);
     for (int k = 0; k < SIMD; k++) memcpy(out + k * N, o[k].data(), N * 8);
   })
 }

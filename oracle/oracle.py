@@ -80,6 +80,8 @@ def _declare(L):
     L.orc_db_reply_a_ntt.argtypes = [c.c_void_p, c.c_int, c.c_void_p]
     L.orc_db_get_a.argtypes = [c.c_void_p, c.c_void_p]
     L.orc_db_perform_pir_split.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
+    L.orc_db_set_db_vec.argtypes = [c.c_void_p, c.c_void_p]
+    L.orc_db_perform_pir_split_vec.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
     L.orc_perform_double_pir.argtypes = [c.c_void_p, c.c_uint32, c.c_uint32] + [c.c_void_p] * 6
     L.orc_condense.argtypes = [c.c_int, c.c_void_p, c.c_uint64, c.c_void_p, _p(c.c_uint64)]
     L.orc_uncondense.argtypes = [c.c_int, c.c_uint64, c.c_void_p, c.c_uint64, c.c_void_p, _p(c.c_uint64)]
@@ -217,6 +219,23 @@ class Database:
         e = np.ascontiguousarray(entries, dtype=np.uint16)
         assert e.shape == (8 * self.l, self.n)
         _check(lib().orc_db_set_db(self._h, _ptr(e)))
+
+    def set_db_vec(self, entries):
+        """set_db through the AVX-512 restatement (8 lanes per vector, the
+        reference's simd_zn.rs shape); the same arrays as set_db."""
+        e = np.ascontiguousarray(entries, dtype=np.uint16)
+        assert e.shape == (8 * self.l, self.n)
+        _check(lib().orc_db_set_db_vec(self._h, _ptr(e)))
+
+    def perform_pir_split_vec(self, qry_b, qry_conj_b, gk_b):
+        """perform_pir_split with the AVX-512 scan."""
+        qb = np.ascontiguousarray(qry_b, dtype=np.int64)
+        qc = None if qry_conj_b is None else np.ascontiguousarray(qry_conj_b, dtype=np.int64)
+        gk = np.ascontiguousarray(gk_b, dtype=np.int64)
+        out = np.zeros((8, self.n), dtype=np.int64)
+        _check(lib().orc_db_perform_pir_split_vec(self._h, _ptr(qb), None if qc is None else _ptr(qc), _ptr(gk),
+                                                  _ptr(out)))
+        return out
 
     def set_transformed_entries(self, entries):
         e = np.ascontiguousarray(entries, dtype=np.uint16)

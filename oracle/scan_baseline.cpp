@@ -29,6 +29,9 @@ extern "C" int orc_db_set_db(void* d, const uint16_t* entries);
 extern "C" int orc_db_perform_pir_split(void* d, const int64_t* qry_b, const int64_t* qry_conj_b, const int64_t* gk_b,
                                         int64_t* out);
 extern "C" int orc_db_get_a(void* d, int64_t* out);
+extern "C" int orc_db_set_db_vec(void* d, const uint16_t* entries);
+extern "C" int orc_db_perform_pir_split_vec(void* d, const int64_t* qry_b, const int64_t* qry_conj_b,
+                                            const int64_t* gk_b, int64_t* out);
 
 namespace {
 
@@ -177,7 +180,8 @@ double orc_scan_baseline(int log2n, uint32_t l, uint32_t shards, int threads, in
 // k mod distinct, as bench_wrapped_pir's preprocessed-db-count does,
 // pir_wrapper.rs:578), run in parallel over (shard, prime, half) units on all
 // threads, then the secondary phase (set_db of the per-query database and its
-// scan, double_pir.rs:195-218) on the oracle.
+// scan, double_pir.rs:195-218) on the oracle library's vectorised restatement
+// (the scalar oracle without AVX-512).
 struct orc_bench {
   int log2n = 11;
   uint32_t l1 = 0, l2 = 0, shards = 0, distinct = 0;
@@ -269,9 +273,13 @@ int orc_bench_step(orc_bench* b, int threads, double* scan_s, double* sec_s, int
   void* db = nullptr;
   int rc = orc_db_create(b->log2n, b->l2, 1, &db);
   std::vector<int64_t> q(8 * b->N, 1), gk(16 * b->N, 1), out(8 * b->N);
-  if (!rc) rc = orc_db_set_db(db, b->sec_entries.data());
+  // the secondary phase on the vectorised restatement (8 lanes per AVX-512
+  // register and the reference's thread split), else on the scalar oracle
+  if (!rc) rc = avx ? orc_db_set_db_vec(db, b->sec_entries.data()) : orc_db_set_db(db, b->sec_entries.data());
   if (!rc) rc = orc_db_get_a(db, out.data());
-  if (!rc) rc = orc_db_perform_pir_split(db, q.data(), b->l2 == b->N ? q.data() : nullptr, gk.data(), out.data());
+  if (!rc)
+    rc = avx ? orc_db_perform_pir_split_vec(db, q.data(), b->l2 == b->N ? q.data() : nullptr, gk.data(), out.data())
+             : orc_db_perform_pir_split(db, q.data(), b->l2 == b->N ? q.data() : nullptr, gk.data(), out.data());
   auto t2 = std::chrono::steady_clock::now();
   if (db) orc_db_free(db);
   if (scan_s) *scan_s = std::chrono::duration<double>(t1 - t0).count();

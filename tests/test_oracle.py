@@ -249,3 +249,28 @@ def test_rng_is_chacha12_stream():
     x = a.next_u64()
     w1, w2 = b.next_u32(), b.next_u32()
     assert x == w1 | (w2 << 32)
+
+
+@pytest.mark.skipif(not orc.cpu_has_avx512(), reason="the vectorised restatement needs AVX-512")
+@pytest.mark.parametrize("log2n,l,used_seeds", [(8, 256, 1), (8, 32, 1), (8, 128, 0), (11, 2048, 1)])
+def test_vectorised_restatement_equals_scalar_oracle(log2n, l, used_seeds):
+    # the AVX-512 restatement the CPU arm times (8 lanes per vector, as the
+    # reference's simd_zn.rs) builds the same arrays as the scalar oracle --
+    # transformed entries, both key digits of every chain step, reply_a -- and
+    # answers perform_pir_split identically
+    n = 1 << log2n
+    gen = np.random.default_rng(40 + l + log2n)
+    data = gen.integers(0, orc.T, size=(8 * l, n), dtype=np.uint16)
+    a = orc.Database(log2n, l, used_seeds)
+    a.set_db(data)
+    b = orc.Database(log2n, l, used_seeds)
+    b.set_db_vec(data)
+    for which in range(3):
+        for conj in range(2 if l == n else 1):
+            for prime in range(2):
+                assert np.array_equal(a.array(which, conj, prime), b.array(which, conj, prime)), (which, conj, prime)
+    assert np.array_equal(a.get_a(), b.get_a())
+    qb = gen.integers(0, orc.Q, size=(8, n), dtype=np.int64)
+    qc = gen.integers(0, orc.Q, size=(8, n), dtype=np.int64) if l == n else None
+    gk = gen.integers(0, orc.Q, size=(8, 2, n), dtype=np.int64)
+    assert np.array_equal(a.perform_pir_split(qb, qc, gk), b.perform_pir_split_vec(qb, qc, gk))
