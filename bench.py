@@ -146,14 +146,17 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name):
-    """dram bytes per launch from a committed ncu summary (profiles/<name>), or None."""
+def profiled_traffic(name, algo_bytes):
+    """dram bytes per launch from a committed ncu summary (profiles/<name>):
+    its measured ratio of dram bytes to algorithmic bytes (the captured launch
+    reads each slab block once, so traffic grows with the slabs) times this
+    launch's algorithmic bytes; None without a summary."""
     p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
-            m = re.match(r"\s*traffic_bytes_per_launch_full:\s*([0-9.eE+]+)", line)
+            m = re.match(r"\s*traffic_ratio:\s*([0-9.eE+]+)", line)
             if m:
-                return float(m.group(1))
+                return float(m.group(1)) * algo_bytes
     except OSError:
         pass
     return None
@@ -900,7 +903,7 @@ def main():
     achieved = algo_bytes / (scan_avg * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     kname = "tscan_kernel" if args.engine == "tensor" else "scan_batch_kernel"
-    traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_batch_2p22.md")
+    traffic = profiled_traffic("tscan_2p22.md" if args.engine == "tensor" else "scan_batch_2p22.md", algo_bytes)
     value = whole_job_rate(args.steps, world, total_ms * 1e-3)
     fleet.close()
     del qdev, rdev
