@@ -146,6 +146,36 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def int8_tensor_peak(torch, dev, n=8192, seconds=1.5):
+    """Sustained int8 tensor throughput of a library GEMM on this GPU: cuBLASLt
+    through torch._int_mm, n^3 s8 x s8 -> s32, called back to back for about
+    `seconds` (long enough to settle under the power cap, as the batched scan
+    does); the median of the second half's 20-call batches, in POPS (2 ops per
+    MAC).  It is the denominator of the batched scan's tensor fraction; None
+    if the GEMM is unavailable."""
+    try:
+        a = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev)
+        b = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev).t()  # column-major operand
+        torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        rates, t_end = [], time.time() + seconds
+        while time.time() < t_end:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(20):
+                c = torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            rates.append(20 * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e15)
+        del a, b, c
+        torch.cuda.empty_cache()
+        half = rates[len(rates) // 2:]
+        return {"pops": statistics.median(half), "gemm": f"torch._int_mm (cuBLASLt) {n}x{n}x{n} int8 -> int32",
+                "batches": len(rates), "seconds": seconds}
+    except Exception as e:  # noqa: BLE001 -- reported, not fatal
+        return {"pops": None, "error": str(e).splitlines()[0][:200]}
+
+
 def profiled_traffic(name, algo_bytes):
     """dram bytes per launch from a committed ncu summary (profiles/<name>):
     its measured ratio of dram bytes to algorithmic bytes (the captured launch
@@ -909,6 +939,11 @@ def main():
     del qdev, rdev
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
+    int8_peak = None
+    if args.engine == "tensor" and batched:
+        int8_peak = int8_tensor_peak(torch, dev)
+        for v in batched.values():
+            v["scan_tensor_frac"] = (v["scan_tensor_pops"] / int8_peak["pops"]) if int8_peak["pops"] else None
     legs = {}
     if not args.quick and world == 1:
         legs = extra_legs(args, dp, torch, dev, local_rank)
@@ -934,6 +969,9 @@ def main():
         "engine": args.engine,
         "batched": batched,
         "batched_vs_plain": {b: v["responses_per_sec"] / value for b, v in batched.items()},
+        "int8_tensor_peak": int8_peak,
+        "int8_tensor_peak_note": "scan_tensor_frac of each group size = scan_tensor_pops / this library GEMM's "
+                                 "sustained int8 rate, measured in the same run",
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": algo_bytes},
@@ -947,6 +985,9 @@ def main():
         "checked": {"decrypted_ok": ok, "of": args.steps},
     }
     check1 = legs.pop("_config1_check", None)
+    if int8_peak and int8_peak["pops"] and "config4" in legs:
+        for v in legs["config4"]["groups"].values():
+            v["scan_tensor_frac"] = v["scan_tensor_pops"] / int8_peak["pops"]
     line.update(legs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_line(args, l1, l2, shards)
