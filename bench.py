@@ -146,34 +146,52 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def _gemm_rate(torch, fn, n, seconds):
+    """Median rate (POPS, 2 ops per MAC) of the second half of 20-call
+    batches of an n^3 GEMM called back to back for about `seconds`."""
+    fn()
+    torch.cuda.synchronize()
+    rates, t_end = [], time.time() + seconds
+    while time.time() < t_end:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            fn()
+        e1.record()
+        e1.synchronize()
+        rates.append(20 * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e15)
+    return statistics.median(rates[len(rates) // 2:]), len(rates)
+
+
 def int8_tensor_peak(torch, dev, n=8192, seconds=1.5):
-    """Sustained int8 tensor throughput of a library GEMM on this GPU: cuBLASLt
-    through torch._int_mm, n^3 s8 x s8 -> s32, called back to back for about
-    `seconds` (long enough to settle under the power cap, as the batched scan
-    does); the median of the second half's 20-call batches, in POPS (2 ops per
-    MAC).  It is the denominator of the batched scan's tensor fraction; None
-    if the GEMM is unavailable."""
+    """Sustained 8-bit tensor throughput of library GEMMs on this GPU, the
+    denominator of the batched scan's tensor fraction: cuBLASLt through
+    torch._int_mm (n^3, s8 x s8 -> s32) and through torch._scaled_mm (n^3,
+    e4m3 x e4m3 -> bf16, the same nominal tensor rate), each called back to
+    back for about `seconds` (long enough to settle under the power cap, as
+    the batched scan does).  `pops` is the faster of the two; None if neither
+    GEMM is available."""
+    out = {"gemm_n": n, "seconds": seconds}
     try:
         a = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev)
         b = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev).t()  # column-major operand
-        torch._int_mm(a, b)
-        torch.cuda.synchronize()
-        rates, t_end = [], time.time() + seconds
-        while time.time() < t_end:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(20):
-                c = torch._int_mm(a, b)
-            e1.record()
-            e1.synchronize()
-            rates.append(20 * 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e15)
-        del a, b, c
-        torch.cuda.empty_cache()
-        half = rates[len(rates) // 2:]
-        return {"pops": statistics.median(half), "gemm": f"torch._int_mm (cuBLASLt) {n}x{n}x{n} int8 -> int32",
-                "batches": len(rates), "seconds": seconds}
+        out["int8_pops"], _ = _gemm_rate(torch, lambda: torch._int_mm(a, b), n, seconds)
+        del a, b
     except Exception as e:  # noqa: BLE001 -- reported, not fatal
-        return {"pops": None, "error": str(e).splitlines()[0][:200]}
+        out["int8_error"] = str(e).splitlines()[0][:200]
+    try:
+        a = torch.randn(n, n, device=dev).to(torch.float8_e4m3fn)
+        b = torch.randn(n, n, device=dev).to(torch.float8_e4m3fn).t()
+        one = torch.ones((), device=dev)
+        out["fp8_pops"], _ = _gemm_rate(
+            torch, lambda: torch._scaled_mm(a, b, scale_a=one, scale_b=one, out_dtype=torch.bfloat16), n, seconds)
+        del a, b
+    except Exception as e:  # noqa: BLE001
+        out["fp8_error"] = str(e).splitlines()[0][:200]
+    torch.cuda.empty_cache()
+    rates = [out[k] for k in ("int8_pops", "fp8_pops") if k in out]
+    out["pops"] = max(rates) if rates else None
+    return out
 
 
 def profiled_traffic(name, algo_bytes):
@@ -970,8 +988,8 @@ def main():
         "batched": batched,
         "batched_vs_plain": {b: v["responses_per_sec"] / value for b, v in batched.items()},
         "int8_tensor_peak": int8_peak,
-        "int8_tensor_peak_note": "scan_tensor_frac of each group size = scan_tensor_pops / this library GEMM's "
-                                 "sustained int8 rate, measured in the same run",
+        "int8_tensor_peak_note": "scan_tensor_frac of each group size = scan_tensor_pops / the faster of two "
+                                 "library 8-bit GEMMs (cuBLASLt int8 and fp8), sustained, measured in the same run",
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": algo_bytes},

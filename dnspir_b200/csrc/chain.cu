@@ -840,8 +840,7 @@ __global__ void __launch_bounds__(CT, 1) secondary_chain2k_kernel(ChainArgs a) {
       ct(v.y, v.w, w.a, w.aq, p);
       ct(v.x, v.y, w.b0, w.b0q, p);
       ct(v.z, v.w, w.b1, w.b1q, p);
-      const uint32_t n1s[4] = {red(red(v.x, 2 * p), p), red(red(v.y, 2 * p), p), red(red(v.z, 2 * p), p),
-                               red(red(v.w, 2 * p), p)};
+      const uint32_t n1s[4] = {canon(v.x, p), canon(v.y, p), canon(v.z, p), canon(v.w, p)};
       const uint4 e = h4 ? e1 : e0;
       const uint32_t es[4] = {e.x, e.y, e.z, e.w};
       uint32_t kc[6][4];

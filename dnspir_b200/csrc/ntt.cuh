@@ -34,17 +34,26 @@ __device__ __forceinline__ uint32_t prime_of(int pi) { return pi ? P2 : P1; }
 
 namespace ntt_detail {
 
-// Harvey's lazy butterflies with Shoup multiplication: a forward pass keeps
-// values in [0, 4p), an inverse pass in [0, 2p) (4p < 2^28).
+// Lazy butterflies with Shoup multiplication.  Inverse (Gentleman-Sande, as
+// Harvey): values stay in [0, 2p).  Forward (Cooley-Tukey): the multiplied
+// operand is brought to [0, 2p) by the Shoup product and nothing else is
+// reduced, so each stage adds at most 2p to the bound of its outputs; a
+// transform of at most 11 stages on inputs below 4p ends below 26p < 2^31
+// (p < 2^26), and canon() brings the results to [0, p).
 __device__ __forceinline__ uint32_t lazy_mul(uint32_t x, uint32_t w, uint32_t wq, uint32_t p) {
   return x * w - __umulhi(x, wq) * p;  // in [0, 2p) for any x < 2^32
 }
 __device__ __forceinline__ uint32_t red(uint32_t x, uint32_t m) { return x >= m ? x - m : x; }
+// x mod p for any x < 2^32, p in {q1, q2}: the Shoup product x * 1 (companion
+// floor(2^32 / p)) lands in [0, 2p), one conditional subtraction finishes
+__device__ __forceinline__ uint32_t canon(uint32_t x, uint32_t p) {
+  constexpr uint32_t ONE_Q1 = (uint32_t)((1ull << 32) / P1), ONE_Q2 = (uint32_t)((1ull << 32) / P2);
+  return red(lazy_mul(x, 1u, p == P1 ? ONE_Q1 : ONE_Q2, p), p);
+}
 __device__ __forceinline__ void ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
-  const uint32_t a = red(x, 2 * p);
   const uint32_t t = lazy_mul(y, w, wq, p);
-  x = a + t;
-  y = a - t + 2 * p;
+  y = x - t + 2 * p;
+  x = x + t;
 }
 __device__ __forceinline__ void gs(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
   const uint32_t a = x + y;
@@ -94,14 +103,14 @@ __device__ __forceinline__ void fwd_t(uint32_t* x, int logn_rt, int cnt0, int cn
       uint32_t* a = x + (poly << logn) + 2 * b;
       uint32_t u = a[0], v = a[1];
       ct(u, v, __ldg(T.fw[pi] + n / 2 + b), __ldg(T.fwq[pi] + n / 2 + b), p);
-      a[0] = red(red(u, 2 * p), p);
-      a[1] = red(red(v, 2 * p), p);
+      a[0] = canon(u, p);
+      a[1] = canon(v, p);
     }
   } else {
     const int total = cnt << logn;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
       const uint32_t p = prime_of((b >> logn) >= cnt0);
-      x[b] = red(red(x[b], 2 * p), p);
+      x[b] = canon(x[b], p);
     }
   }
   __syncthreads();

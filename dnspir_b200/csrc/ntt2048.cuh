@@ -29,6 +29,7 @@ constexpr int PS = N + N / 8;  // padded words per polynomial
 __host__ __device__ __forceinline__ constexpr uint32_t phys(uint32_t i) { return i + ((i >> 5) << 2); }
 __device__ __forceinline__ uint32_t brv11(uint32_t i) { return __brev(i) >> 21; }
 
+using ntt_detail::canon;
 using ntt_detail::ct;
 using ntt_detail::gs;
 using ntt_detail::lazy_mul;
@@ -208,9 +209,7 @@ __device__ __forceinline__ void pass4(uint32_t* x, int cnt0, int cnt1, const Ntt
           ct(v.y, v.w, a, aq, p);
           ct(v.x, v.y, b0, b0q, p);
           ct(v.z, v.w, b1, b1q, p);
-          const uint32_t p2 = 2 * p;
-          v.x = red(red(v.x, p2), p), v.y = red(red(v.y, p2), p);
-          v.z = red(red(v.z, p2), p), v.w = red(red(v.w, p2), p);
+          v.x = canon(v.x, p), v.y = canon(v.y, p), v.z = canon(v.z, p), v.w = canon(v.w, p);
         }
         *y = v;
       }

@@ -163,14 +163,16 @@ __device__ __forceinline__ void limb_weights(uint32_t pr, uint64_t mu, int k, ui
 // recombined with the weights c and reduced mod pr; lanes 4 l8 .. 4 l8 + 3
 // hold the four limbs k of SIMD lane l8, so three of every four lanes sum the
 // others' partial recombinations with shuffles and lane k keeps query
-// 4 q4 + k's sum.  Columns are read 64 (16 for NQ = 16) per TMEM load.
+// 4 q4 + k's sum.  The warp reads columns c_lo .. c_hi - 1 (multiples of the
+// load width), 64 (16 for NQ = 16) per TMEM load.
 template <int NQ>
 __device__ __forceinline__ void epilogue_tile(const TScanArgs& a, uint32_t taddr, const uint32_t (&c)[4], uint32_t pr,
-                                              uint64_t mu, uint32_t grp, uint32_t u, int s, int p, int k, int l8) {
+                                              uint64_t mu, uint32_t grp, uint32_t u, int s, int p, int k, int l8,
+                                              int c_lo = 0, int c_hi = NQ) {
   constexpr int CW = NQ >= 64 ? 64 : 16;  // columns per TMEM load
   const uint32_t N = 2 * a.half;
 #pragma unroll 1
-  for (int c0 = 0; c0 < NQ; c0 += CW) {
+  for (int c0 = c_lo; c0 < c_hi; c0 += CW) {
     uint32_t v[CW];
     if constexpr (CW == 64)
       tmem_ld64(taddr + c0, v);
@@ -329,20 +331,31 @@ __global__ void __launch_bounds__(TSCAN_NT, 1) tscan_kernel(TScanArgs a) {
 // ---- persistent, warp-specialised variant.  Warp 0 streams the A and V
 // chunks of every tile the CTA owns (tiles blockIdx.x, + gridDim.x, ...)
 // through the stage ring; warp 1 issues the MMAs of tile j into TMEM
-// accumulator j mod 2; warps 2..5 read accumulator j mod 2 (TMEM lane quarter
-// warp mod 4) and write the residues, then release it, so the epilogue of
-// tile j overlaps the main loop of tile j + 1.  Needs 2 x MTPC x NQ <= 512
-// TMEM columns.  Waits are bounded as in tscan_kernel; a role that gives up
-// raises the abort flag, and the CTA still waits for its MMAs and copies in
-// flight before it frees TMEM.
-constexpr int TSCANP_NT = 192;
+// accumulator j mod 2; warps 2 .. 2 + 4 EW - 1 read accumulator j mod 2 (TMEM
+// lane quarter warp mod 4; the EW warps of a quarter split the columns, 64
+// each) and write the residues, then release it, so the epilogue of tile j
+// overlaps the main loop of tile j + 1.  With 2 x MTPC x NQ > 512 TMEM columns
+// there is one accumulator and the MMAs of a tile wait for the previous
+// tile's epilogue: the EW warps per quarter keep that wait short (one warp per
+// quarter leaves each scheduler one dependent chain of TMEM loads, shuffles
+// and reductions).  Waits are bounded as in tscan_kernel; a role that gives
+// up raises the abort flag, and the CTA still waits for its MMAs and copies
+// in flight before it frees TMEM.
+template <int NQ>
+constexpr int tscanp_ew() {
+  return NQ >= 256 ? 4 : NQ >= 128 ? 2 : 1;
+}
+template <int NQ>
+constexpr int tscanp_nt() {
+  return 64 + 128 * tscanp_ew<NQ>();
+}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(bar)) : "memory");
 }
 
 template <int NQ, int MTPC>
-__global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
+__global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscanp_kernel(TScanArgs a) {
   constexpr uint32_t A_BYTES = MTPC * TBLK;
   constexpr uint32_t STAGE = A_BYTES + NQ * 128;
   constexpr uint32_t ACC = MTPC * NQ;  // TMEM columns of one accumulator
@@ -350,7 +363,9 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
   // a tile wait for the previous tile's epilogue, but its chunks still stream in
   constexpr uint32_t BUFS = 2 * ACC <= 512 ? 2 : 1;
   constexpr uint32_t COLS = BUFS * ACC;
+  constexpr int EW = tscanp_ew<NQ>();  // epilogue warps per TMEM lane quarter
   static_assert(STAGE % 1024 == 0 && ACC >= 16 && COLS <= 512 && (COLS & (COLS - 1)) == 0, "tile shape");
+  static_assert(NQ % EW == 0 && (EW == 1 || NQ / EW == 64), "columns per epilogue warp");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   const uint32_t S_ = a.stages;
@@ -375,7 +390,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 4);
+      mbar_init(&acce[b], 4 * EW);
     }
     mbar_init(done, 1);
     *issued_s = 0;
@@ -476,6 +491,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
   } else {
     const int q = warp & 3;  // TMEM lane quarter = slot e mod 4 of the m-tile
     const int k = lane & 3, l8 = lane >> 2;
+    const int c_lo = ((warp - 2) >> 2) * (NQ / EW);  // this warp's columns of every m-tile
     uint32_t j = 0;
     for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, j++) {
       const uint32_t buf = j % BUFS, use = j / BUFS;
@@ -496,7 +512,7 @@ __global__ void __launch_bounds__(TSCANP_NT, 1) tscanp_kernel(TScanArgs a) {
       limb_weights(pr, mu, k, c);
       for (int t = 0; t < MTPC; t++)
         epilogue_tile<NQ>(a, tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ, c, pr, mu, grp,
-                          sgn * a.half + 4 * (mt0 + t) + q, s, p, k, l8);
+                          sgn * a.half + 4 * (mt0 + t) + q, s, p, k, l8, c_lo, c_lo + NQ / EW);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[buf]);
@@ -908,7 +924,7 @@ int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
   set_smem(tscanp_kernel<NQ, MTPC>, smem);
   constexpr int COLS = (2 * MTPC * NQ <= 512 ? 2 : 1) * MTPC * NQ;
   int per_sm = 0, dev = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tscanp_kernel<NQ, MTPC>, TSCANP_NT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tscanp_kernel<NQ, MTPC>, tscanp_nt<NQ>(), smem);
   // resident CTAs must not ask for more TMEM columns than the SM has (a CTA
   // whose allocation waits would hold its SM until a neighbour finishes)
   if (per_sm < 1 || per_sm * COLS > 512) return -1;
@@ -916,7 +932,7 @@ int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t items = (size_t)a.nshards * 4 * (a.mt_total / MTPC) * a.groups;
   const size_t grid = std::min(items, (size_t)sms * per_sm);
-  tscanp_kernel<NQ, MTPC><<<(unsigned)grid, TSCANP_NT, smem, st>>>(a);
+  tscanp_kernel<NQ, MTPC><<<(unsigned)grid, tscanp_nt<NQ>(), smem, st>>>(a);
   return 0;
 }
 
