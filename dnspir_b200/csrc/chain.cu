@@ -203,15 +203,23 @@ __device__ __forceinline__ void inv_multi(uint32_t* x0, int stride, int logn_rt,
   // outputs are in [0, 2p); the consumer (high_digit via Shoup) accepts any value < 2^32
 }
 
-// high digit of the centred CRT lift from the two factors' unscaled iNTT outputs
+// High digit of the centred CRT lift from the two factors' unscaled iNTT
+// outputs: x = v - k q (v = x1 q2 + x2 q1 < 2q, k = round(v / q)), digit
+// floor((x + 2^25) / 2^26).  Computed in double precision, exactly: x1 q2 and
+// x2 q1 are below 2^51, v below 2^52 and q = q1 q2 below 2^51, so every sum,
+// difference and comparison is exact in the 53-bit significand, and
+// x 2^-26 + 1/2 (a power-of-two scaling of an integer below 2^51 in
+// magnitude, plus one half) is exact too, leaving floor() the only rounding
+// -- the same integer as the 64-bit formula, on the FP64 pipe instead of the
+// integer pipes the transforms saturate.
 __device__ __forceinline__ int32_t high_digit(uint32_t c1, uint32_t c2, const ChainPrime& P1c, const ChainPrime& P2c) {
   const uint32_t x1 = shoup_mul(c1, P1c.k1, P1c.k1q, P1);
   const uint32_t x2 = shoup_mul(c2, P2c.k2, P2c.k2q, P2);
-  uint64_t v = (uint64_t)x1 * P2 + (uint64_t)x2 * P1;
-  v = v >= QQ ? v - QQ : v;
-  int64_t x = (int64_t)v;
-  if (v > QQ / 2) x -= (int64_t)QQ;
-  return (int32_t)((x + ((int64_t)1 << (LOG2_B - 1))) >> LOG2_B);
+  constexpr double Q = (double)QQ, HALF_Q = (double)(QQ / 2);  // QQ / 2 = (q - 1) / 2, exact
+  double v = fma((double)x1, (double)P2, (double)x2 * (double)P1);
+  v = v >= Q ? v - Q : v;
+  v = v > HALF_Q ? v - Q : v;
+  return __double2int_rd(fma(v, 1.0 / (double)(1u << LOG2_B), 0.5));
 }
 
 struct ChainArgs {

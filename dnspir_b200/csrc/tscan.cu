@@ -64,12 +64,26 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// The same test, but a thread whose phase is not complete may stay suspended
+// up to hint_ns (instead of the system's shorter default) before it returns
+// false: long waits (an epilogue warp waiting out a tile's MMAs) then issue
+// almost nothing while they wait.
+__device__ __forceinline__ bool mbar_try_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(sa(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+constexpr uint32_t SLEEP_HINT_NS = 20000;
 
 // Wait for the phase of `parity` to complete; false after limit_ns.
 __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = gtimer();
-  while (!mbar_try(bar, parity))
+  while (!mbar_try_sleep(bar, parity, SLEEP_HINT_NS))
     if (gtimer() - t0 > limit_ns) return false;
   return true;
 }
