@@ -96,39 +96,19 @@ __device__ __forceinline__ void fwd8_bf(uint32_t (&v)[8], const Tw8& t, uint32_t
   ct(v[4], v[5], t.c[2], t.cq[2], p);
   ct(v[6], v[7], t.c[3], t.cq[3], p);
 }
-// Gentleman-Sande butterfly without the reduction of the sum: (x, y) ->
-// (x + y, w (x - y + YB p)), YB p a bound of y, so x - y + YB p is never
-// negative; the product is in [0, 2p).
-template <int YB>
-__device__ __forceinline__ void gs_open(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p) {
-  const uint32_t d = x - y + YB * p;
-  x = x + y;
-  y = lazy_mul(d, w, wq, p);
-}
-// Three inverse stages on 8 values of any size below 2^32: each is first
-// brought to [0, 2p) by the Shoup product with 1, then only the products are
-// reduced.  Following the bounds through the stages (in units of p): after
-// the first, the sums v0 v2 v4 v6 < 4; after the second, v0 v4 < 8 and
-// v1 v5 < 4; after the third v0 < 16, v1 < 8, v2 v3 < 4 and the rest < 2.
-// Every value stays below 16p < 2^31, and every consumer of an inverse pass
-// (the next pass, the scaling by N^-1, the CRT digit) reduces with a Shoup
-// product, which takes any value below 2^32.
 __device__ __forceinline__ void inv8_bf(uint32_t (&v)[8], const Tw8& t, uint32_t p) {
-  const uint32_t one_q = p == P1 ? (uint32_t)((1ull << 32) / P1) : (uint32_t)((1ull << 32) / P2);
-#pragma unroll
-  for (int k = 0; k < 8; k++) v[k] = lazy_mul(v[k], 1u, one_q, p);
-  gs_open<2>(v[0], v[1], t.c[0], t.cq[0], p);
-  gs_open<2>(v[2], v[3], t.c[1], t.cq[1], p);
-  gs_open<2>(v[4], v[5], t.c[2], t.cq[2], p);
-  gs_open<2>(v[6], v[7], t.c[3], t.cq[3], p);
-  gs_open<4>(v[0], v[2], t.b[0], t.bq[0], p);
-  gs_open<2>(v[1], v[3], t.b[0], t.bq[0], p);
-  gs_open<4>(v[4], v[6], t.b[1], t.bq[1], p);
-  gs_open<2>(v[5], v[7], t.b[1], t.bq[1], p);
-  gs_open<8>(v[0], v[4], t.a, t.aq, p);
-  gs_open<4>(v[1], v[5], t.a, t.aq, p);
-  gs_open<2>(v[2], v[6], t.a, t.aq, p);
-  gs_open<2>(v[3], v[7], t.a, t.aq, p);
+  gs(v[0], v[1], t.c[0], t.cq[0], p);
+  gs(v[2], v[3], t.c[1], t.cq[1], p);
+  gs(v[4], v[5], t.c[2], t.cq[2], p);
+  gs(v[6], v[7], t.c[3], t.cq[3], p);
+  gs(v[0], v[2], t.b[0], t.bq[0], p);
+  gs(v[1], v[3], t.b[0], t.bq[0], p);
+  gs(v[4], v[6], t.b[1], t.bq[1], p);
+  gs(v[5], v[7], t.b[1], t.bq[1], p);
+  gs(v[0], v[4], t.a, t.aq, p);
+  gs(v[1], v[5], t.a, t.aq, p);
+  gs(v[2], v[6], t.a, t.aq, p);
+  gs(v[3], v[7], t.a, t.aq, p);
 }
 
 // Default end of an inverse transform: scale by N^-1 into [0, p), in place.
@@ -251,7 +231,7 @@ __device__ __forceinline__ void fwd(uint32_t* x, int cnt0, int cnt1, const NttTa
 
 // Inverse transform (canonical input at transform positions).  The last pass
 // hands each thread's 8 values -- logical words r + 256 k of polynomial poly,
-// unscaled, below 16p -- to fin(y, poly, r, v, p, N^-1, its Shoup companion),
+// unscaled, in [0, 2p) -- to fin(y, poly, r, v, p, N^-1, its Shoup companion),
 // y pointing at word r of the polynomial (stride Geo8<1>::STR); the default
 // stores them scaled into [0, p).
 template <int NT, class Fin = ScaleStore>
