@@ -50,6 +50,7 @@ cores, rank 0 only: every step is one whole query (all shards scanned, then
 the secondary phase), timed for real.
 """
 import argparse
+import datetime
 import hashlib
 import json
 import os
@@ -86,7 +87,8 @@ def parse():
     ap.add_argument("--engine", default="tensor", choices=["tensor", "cuda"])
     ap.add_argument("--batched", default="16,64,128,256", help="comma-separated group sizes measured after the plain run")
     ap.add_argument("--quick", action="store_true", help="skip the 2^20 and served-mix legs")
-    ap.add_argument("--tile", default="", help="B:shape,... force a tensor tile shape for group size B (no tuning)")
+    ap.add_argument("--tile", default="", help="B:shape[:schedule],... force a tensor tile shape (and pipeline "
+                    "schedule) for group size B (no tuning)")
     ap.add_argument("--cpu-distinct", type=int, default=4, help="distinct shard slabs in host RAM for the CPU arm")
     ap.add_argument("--batched-groups", type=int, default=3, help="timed groups per batched size")
     ap.add_argument("--reserve-gib", type=float, default=0.0, help="HBM left free for workspaces (0: from the group sizes)")
@@ -211,9 +213,13 @@ def profiled_traffic(name, algo_bytes):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms.  It is
+    started before the warm-up (its own start-up, which queries the driver,
+    stays out of the timed region) and stopped after; stop() keeps the samples
+    whose timestamps fall inside the timed region (host clock), or the one
+    nearest to it when the region is shorter than a sampling period."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -222,15 +228,19 @@ class ClockSampler:
         self.proc = None
         self.out = tempfile.NamedTemporaryFile(prefix="clocks", suffix=".csv", delete=False)
 
-    def start(self):
+    def start(self, settle_s=3.0):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t_end = time.time() + settle_s  # until the first sample is written
+        while time.time() < t_end and os.path.getsize(self.out.name) == 0:
+            time.sleep(0.05)
 
-    def stop(self):
+    def stop(self, window=None):
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -242,18 +252,30 @@ class ClockSampler:
         try:
             for line in open(self.out.name):
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
+                if len(parts) >= 10:
+                    try:
+                        parts[0] = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        continue
                     rows.append(parts)
         finally:
             os.unlink(self.out.name)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        where = "timed region"
+        if window is not None:
+            inside = [r for r in rows if window[0] - 0.1 <= r[0] <= window[1] + 0.1]
+            if not inside:
+                mid = 0.5 * (window[0] + window[1])
+                inside = [min(rows, key=lambda r: abs(r[0] - mid))]
+                where = "nearest sample to the timed region"
+            rows = inside
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        smax = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "sampled": where}
 
 
 def pack_host(payload):
@@ -811,6 +833,8 @@ def main():
     for w in range(args.warmup):
         fleet.process_queries_device(qdev[w:w + 1], rdev[w:w + 1])
     unloaded = []
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     for w in range(args.warmup):
         fleet.process_queries_device(qdev[w:w + 1], rdev[w:w + 1])
         unloaded.append(fleet.batch_timings(1)[0, 0])
@@ -820,20 +844,20 @@ def main():
     # (the primary phase of query k+1 overlaps the secondary phase of query k)
     barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     w0 = args.warmup
     launches0 = fleet.launch_count()
+    t_timed0 = time.time()
     ev0.record(stream)
     fleet.process_queries_device(qdev[w0:w0 + args.steps], rdev[w0:w0 + args.steps])
     ev1.record(stream)
     launches = fleet.launch_count() - launches0
     torch.cuda.synchronize()
+    t_timed1 = time.time()
     barrier()
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop((t_timed0, t_timed1))
     total_ms = max_over_ranks(ev0.elapsed_time(ev1))
     tim = fleet.batch_timings(args.steps)
     step_ms = list(tim[0])
@@ -884,13 +908,18 @@ def main():
             pq.append(q)
             pseeds.append(sk)
         pdev = torch.tensor(np.frombuffer(b"".join(pq), dtype=np.uint8).reshape(pool_n, qlen), device=dev)
-        forced = {int(a): int(b) for a, b in (x.split(":") for x in args.tile.split(",") if x.strip())}
+        # --tile B:shape[:schedule]
+        forced = {int(f[0]): [int(x) for x in f[1:]] for f in (x.split(":") for x in args.tile.split(",") if x.strip())}
         for B in sizes:
             shape = None
             if args.engine == "tensor" and B in forced:
-                fleet.set_tile(B, forced[B])
-                sh = dp.tscan_shapes()[forced[B]]
+                fleet.set_tile(B, forced[B][0])
+                if len(forced[B]) > 1:
+                    fleet.set_schedule(B, forced[B][1])
+                sh = dp.tscan_shapes()[forced[B][0]]
                 shape = {"rows_per_cta": sh[0], "mtiles_per_cta": sh[1], "stages": sh[2], "persistent": bool(sh[3]),
+                         "schedule": {"order": ("overlap", "serial", "last chunk")[fleet.get_schedule(B) & 3],
+                                      "cluster_chains": bool(fleet.get_schedule(B) & 4)},
                          "tuner": "forced (--tile)"}
             elif args.engine == "tensor":
                 ch, tms, shapes = fleet.tune(B, pipeline=True)

@@ -82,7 +82,7 @@ __device__ __forceinline__ uint64_t crt(uint32_t c1, uint32_t c2, CrtConst cc) {
 // value mod 2^bits; q is odd, so no ties occur.)  A double estimate is
 // corrected exactly with 128-bit integers.
 __device__ __forceinline__ uint32_t ms_encode(uint64_t v, int bits) {
-  double est = (double)v * (double)(1ull << bits) / (double)QQ;
+  double est = (double)v * ((double)(1ull << bits) * (1.0 / (double)QQ));  // within one of the result
   int64_t r = (int64_t)floor(est + 0.5);
   unsigned __int128 num = ((unsigned __int128)v << (bits + 1)) + QQ;
   unsigned __int128 two_q = (unsigned __int128)(2 * QQ);

@@ -228,10 +228,12 @@ __global__ void primary_epilogue_kernel(const uint32_t* __restrict__ fin, int ns
 constexpr int EPI_NT = 512;
 
 __device__ __forceinline__ uint32_t ms_encode12(uint64_t v) {
-  // round(v 2^12 / q) = floor((v 2^13 + q) / 2q): a double estimate, then
-  // one exact correction (r <= 2^12, so r 2q < 2^64)
+  // round(v 2^12 / q) = floor((v 2^13 + q) / 2q): a double estimate (v times
+  // the rounded constant 2^12 / q, within one of the result), then one exact
+  // correction (r <= 2^12, so r 2q < 2^64)
+  constexpr double SCALE = (double)(1u << PRIM_B_BITS) / (double)QQ;
   const uint64_t num = (v << (PRIM_B_BITS + 1)) + QQ;
-  int64_t r = (int64_t)floor((double)v * (double)(1u << PRIM_B_BITS) / (double)QQ + 0.5);
+  int64_t r = (int64_t)floor((double)v * SCALE + 0.5);
   r = r < 0 ? 0 : r;
   const uint64_t lo = (uint64_t)r * (2 * QQ);
   if (num < lo) r--;

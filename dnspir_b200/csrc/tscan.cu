@@ -558,14 +558,14 @@ __global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscanp_kernel(TScanArgs a)
 // holds more chunks.  Roles, in each CTA: warp 0 lane 0 streams the CTA's
 // chunks into its ring (bulk copies, local full barrier); warp 1 lane 0 is the
 // MMA issuer in the leader and, in the follower, the relay that forwards each
-// completed stage to the leader's pfull barrier; warps 2-5 read the TMEM
-// accumulators and write the residues.  The leader's commits arrive on both
+// completed stage to the leader's pfull barrier; the 4 EW warps after them
+// read the TMEM accumulators and write the residues (EW per lane quarter, as
+// in tscanp_kernel).  The leader's commits arrive on both
 // CTAs' barriers (multicast commit); the epilogue warps of both CTAs release
 // an accumulator on the leader's acce barrier.  Accumulators are
 // double-buffered when 2 MTPC NQ <= 512 TMEM columns.  Every wait is bounded
 // and also gives up once either CTA has raised the pair's abort flag; a CTA
 // then waits (bounded) for its MMAs and copies in flight before it frees TMEM.
-constexpr int TSCAN2_NT = 192;
 
 __device__ __forceinline__ uint32_t cluster_rank() {
   uint32_t r;
@@ -643,7 +643,8 @@ __device__ __forceinline__ void mma2_commit_both(uint64_t* bar) {
 }
 
 template <int NQ, int MTPC>
-__global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
+__global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(TScanArgs a) {
+  constexpr int EW = tscanp_ew<NQ>();  // epilogue warps per TMEM lane quarter, as in tscanp_kernel
   constexpr uint32_t A_BYTES = MTPC * TBLK;
   constexpr uint32_t V_BYTES = NQ / 2 * 128;  // this CTA's half of the group's query rows
   constexpr uint32_t STAGE = A_BYTES + V_BYTES;
@@ -659,7 +660,7 @@ __global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
   uint64_t* empty = full + S_;
   uint64_t* pfull = empty + S_;  // leader: the follower's stage landed
   uint64_t* accf = pfull + S_;   // [2] accumulator ready (multicast commit)
-  uint64_t* acce = accf + 2;     // [2] accumulator drained (leader: 4 local + 4 remote warps)
+  uint64_t* acce = accf + 2;     // [2] accumulator drained (leader: 4 EW local + 4 EW remote warps)
   uint64_t* done = acce + 2;     // every MMA of the pair complete (multicast commit)
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   volatile uint32_t* issued_s = tslot + 1;
@@ -679,7 +680,7 @@ __global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 8);
+      mbar_init(&acce[b], 8 * EW);
     }
     mbar_init(done, 1);
     *issued_s = 0;
@@ -790,6 +791,7 @@ __global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
     const int q = warp & 3;  // TMEM lane quarter = slot e mod 4 of the m-tile
     const int k = lane & 3, l8 = lane >> 2;
     const uint32_t acce_leader = peer_addr(&acce[0], 0);
+    const int c_lo = ((warp - 2) >> 2) * (NQ / EW);  // this warp's columns of every m-tile
     uint32_t j = 0;
     for (uint32_t item = cid; item < items; item += ncl, j++) {
       const uint32_t buf = j % BUFS, use = j / BUFS;
@@ -807,7 +809,7 @@ __global__ void __launch_bounds__(TSCAN2_NT, 1) tscan2_kernel(TScanArgs a) {
       limb_weights(pr, mu, k, c);
       for (int t = 0; t < MTPC; t++)
         epilogue_tile<NQ>(a, tmem + ((uint32_t)(32 * q) << 16) + buf * ACC + t * NQ, c, pr, mu, grp,
-                          sgn * a.half + 4 * (mt0 + rank * MTPC + t) + q, s, p, k, l8);
+                          sgn * a.half + 4 * (mt0 + rank * MTPC + t) + q, s, p, k, l8, c_lo, c_lo + NQ / EW);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) {
@@ -965,7 +967,7 @@ int launch_t2(const TScanArgs& a0, int stages, cudaStream_t st) {
   attr[0].val.clusterDim.x = 2;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
-  cfg.blockDim = dim3(TSCAN2_NT);
+  cfg.blockDim = dim3(tscanp_nt<NQ>());
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cfg.attrs = attr;
