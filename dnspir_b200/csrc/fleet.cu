@@ -111,7 +111,7 @@ int launch_scan(dnspir_fleet* f, QSlot& s, int nb, int Bk) {
     if (nb_pad != Bk) return fail(DNSPIR_ERR_BAD_ARG, "tensor scan batch mismatch");
     if (launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, s.qnat.as<uint32_t>(), qv, nb, Bk, f->qb.as<uint8_t>(),
                      s.fin.as<uint32_t>(), f->err_word.as<uint32_t>(), g1, slot_maps(f->ctx, g1.log2n), shape, f->st,
-                     f->limits))
+                     f->limits, f->tmaps.p))
       return fail(DNSPIR_ERR_BAD_ARG, "tensor scan shape does not fit");
     f->launches += 2;  // query operand + scan
     return DNSPIR_OK;
@@ -338,6 +338,13 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
   CKR(f->distinct_dev.ensure(num_shards * sizeof(int)));
   CK(cudaMemcpy(f->slabs_dev.p, ptrs.data(), num_shards * sizeof(uint32_t*), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(f->distinct_dev.p, dist.data(), num_shards * sizeof(int), cudaMemcpyHostToDevice));
+  if (tensor_layout_supported(f->g1)) {
+    // the slabs stay where they are: their tensor maps are made once
+    CKR(f->tmaps.ensure(tscan_slab_map_bytes((int)num_shards)));
+    std::vector<uint8_t*> hp(num_shards);
+    for (uint32_t s = 0; s < num_shards; s++) hp[s] = reinterpret_cast<uint8_t*>(ptrs[s]);
+    if (tscan_slab_maps(hp.data(), (int)num_shards, f->g1, f->tmaps.p) != 0) f->tmaps.release();
+  }
   CKR(f->a_zq.ensure((size_t)num_distinct * SIMD * f->g1.n * 8));
   CKR(f->a_ms.ensure((size_t)num_distinct * SIMD * f->g1.n * 4));
   *out = f.release();
@@ -428,7 +435,7 @@ int dnspir_fleet_tune(dnspir_fleet* f, uint32_t batch, double* ms_per_shape, int
         cudaEventRecord(e0, f->st);
         ok = launch_tscan(f->slabs_dev.as<uint8_t*>(), f->S, qnat.as<uint32_t>(), QV_WORDS_PER_QUERY * n, nb, pad,
                           qb.as<uint8_t>(), out.as<uint32_t>(), f->err_word.as<uint32_t>(), g1,
-                          slot_maps(f->ctx, g1.log2n), sh[i], f->st) == 0;
+                          slot_maps(f->ctx, g1.log2n), sh[i], f->st, TScanLimits(), f->tmaps.p) == 0;
         cudaEventRecord(e1, f->st);
         if (ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) {
           if (r > 0) tot += t;  // the first run warms up

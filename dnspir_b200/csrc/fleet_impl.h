@@ -46,6 +46,7 @@ struct dnspir_fleet {
   std::vector<bool> ready;
   uint64_t ap_ver = 0;  // a-parts version every ready shard was preprocessed under
   dnspir::DBuf slabs_dev, distinct_dev, a_zq, a_ms;
+  dnspir::DBuf tmaps;  // tensor maps of the slabs (CTA-pair tensor-map scan); empty when unavailable
   dnspir::EncodeWs ws;
   dnspir::QSlot slot[2];
   dnspir::DBuf secE, chain_out, qzq, reply_zq;  // used by one stream at a time

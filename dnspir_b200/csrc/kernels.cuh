@@ -95,7 +95,7 @@ struct TScanShape {
   int nq;          // rows of the query operand per CTA (4 limbs x queries)
   int mtpc;        // 128-row m-tiles per CTA
   int stages;      // shared-memory pipeline depth
-  int persistent;  // 1: persistent warp-specialised kernel, double-buffered TMEM
+  int persistent;  // 1: persistent warp-specialised kernel; 2: CTA pair (relayed bulk copies); 3: CTA pair (tensor maps)
 };
 int tensor_layout_supported(const Group& g);
 void tensor_dims(const Group& g, uint32_t* mt_total, uint32_t* kc_total);
@@ -113,9 +113,17 @@ struct TScanLimits {
 // qb: tscan_query_bytes of workspace; out as launch_scan_batch; err: one
 // device word set to 1 when a bounded wait gave up.  Returns -1 for a shape
 // that does not fit.
+// slab_maps: tscan_slab_maps of the shards (device), required by the
+// tensor-map pair shapes (persistent 3), which are refused (-1) without it.
 int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int nb, int nb_pad,
                  uint8_t* qb, uint32_t* out, uint32_t* err, const Group& g, const SlotMaps& maps,
-                 const TScanShape& shape, cudaStream_t st, const TScanLimits& lim = TScanLimits());
+                 const TScanShape& shape, cudaStream_t st, const TScanLimits& lim = TScanLimits(),
+                 const void* slab_maps = nullptr);
+// Tensor maps of the shards' tensor-layout slabs (host pointers; one map of
+// tscan_slab_map_bytes(1) bytes per shard) written to dev_maps; -1 when the
+// driver cannot encode them.
+size_t tscan_slab_map_bytes(int nshards);
+int tscan_slab_maps(uint8_t* const* host_slabs, int nshards, const Group& g, void* dev_maps);
 // Per-lane queries (perform_pir_split): qlane [(lane*4 + v)*2 + p][N] natural order;
 // part: [chunk][p][u][lane], chunks = H * R.
 int scan_chunks(const Group& g, int nshards);

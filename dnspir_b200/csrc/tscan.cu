@@ -28,7 +28,13 @@
 // their 32 TMEM lanes and write the reduced residues.  Every wait is bounded;
 // a wait that gives up sets an error word, and the CTA still waits for its
 // copies in flight and frees its TMEM before returning.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <string.h>
+
 #include <algorithm>
+#include <vector>
 
 #include "kernels.cuh"
 
@@ -95,6 +101,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// Tensor-map copy of the box at (x, y) into this CTA's shared memory, issued
+// by either CTA of a pair: the byte count completes on the barrier at
+// shared::cluster address mbar, which .cta_group::2 allows to be the peer's
+// (here always the leader's), so the leader learns of both CTAs' data from
+// one barrier.
+__device__ __forceinline__ void tma_load_pair(void* dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(sa(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -156,6 +175,7 @@ struct TScanArgs {
   uint32_t half, mt_total, kc_total, groups, stages;
   uint64_t wait_ns;   // limit of every pipeline wait
   uint32_t withhold;  // test hook: CTA 0's producer stops before this chunk (~0u: never)
+  const CUtensorMap* tmaps;  // per shard: the slab as rows of 128 bytes (tensor-map pair kernel)
 };
 
 // c_w = 2^(8w) mod p (< 2^26) for w = k .. k + 3: the weights of limb product
@@ -642,8 +662,9 @@ __device__ __forceinline__ void mma2_commit_both(uint64_t* bar) {
       : "memory");
 }
 
-template <int NQ, int MTPC>
-__global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(TScanArgs a) {
+template <int NQ, int MTPC, bool TMA>
+__global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(const __grid_constant__ TScanArgs a,
+                                                                    const __grid_constant__ CUtensorMap qmap) {
   constexpr int EW = tscanp_ew<NQ>();  // epilogue warps per TMEM lane quarter, as in tscanp_kernel
   constexpr uint32_t A_BYTES = MTPC * TBLK;
   constexpr uint32_t V_BYTES = NQ / 2 * 128;  // this CTA's half of the group's query rows
@@ -732,26 +753,42 @@ __global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(TScanArgs a)
             break;
           }
           uint8_t* dst = sm + st * STAGE;
-          mbar_expect_tx(&full[st], STAGE);
+          if constexpr (TMA) {
+            // both CTAs' copies complete on the leader's barrier, which the
+            // leader arms with the pair's bytes (a copy may land before it is
+            // armed: the transaction count may run below zero meanwhile)
+            if (rank == 0) mbar_expect_tx(&full[st], 2 * STAGE);
+            const uint32_t fb = peer_addr(&full[st], 0);
+            const int arow = (int)(((ps * a.mt_total + mt0 + rank * MTPC) * KC + kc) * 128);
 #pragma unroll
-          for (int t = 0; t < MTPC; t++)
-            bulk_g2s(dst + t * TBLK, abase + ((size_t)t * KC + kc) * TBLK, TBLK, &full[st]);
-          bulk_g2s(dst + A_BYTES, bbase + (size_t)kc * a.nq_rows * 128, V_BYTES, &full[st]);
+            for (int t = 0; t < MTPC; t++) tma_load_pair(dst + t * TBLK, a.tmaps + s, 0, arow + t * (int)KC * 128, fb);
+            tma_load_pair(dst + A_BYTES, &qmap, 0,
+                          (int)((ps * KC + kc) * a.nq_rows + (size_t)grp * NQ + rank * (NQ / 2)), fb);
+          } else {
+            mbar_expect_tx(&full[st], STAGE);
+#pragma unroll
+            for (int t = 0; t < MTPC; t++)
+              bulk_g2s(dst + t * TBLK, abase + ((size_t)t * KC + kc) * TBLK, TBLK, &full[st]);
+            bulk_g2s(dst + A_BYTES, bbase + (size_t)kc * a.nq_rows * 128, V_BYTES, &full[st]);
+          }
           *issued_s = g + 1;
         }
       }
     }
   } else if (warp == 1) {
     if (lane == 0 && rank != 0) {
-      // relay: each stage of this CTA that lands is announced to the leader
-      const uint32_t total = ((items > cid ? (items - cid + ncl - 1) / ncl : 0)) * KC;
-      for (uint32_t g = 0; g < total; g++) {
-        const uint32_t st = g % S_, n = g / S_;
-        if (!mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, false)) {
-          if (!*abort_s) pair_abort(abort_s, a.err);
-          break;
+      if constexpr (!TMA) {
+        // relay: each stage of this CTA that lands is announced to the leader
+        // (with tensor-map copies the follower's copies signal the leader)
+        const uint32_t total = ((items > cid ? (items - cid + ncl - 1) / ncl : 0)) * KC;
+        for (uint32_t g = 0; g < total; g++) {
+          const uint32_t st = g % S_, n = g / S_;
+          if (!mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, false)) {
+            if (!*abort_s) pair_abort(abort_s, a.err);
+            break;
+          }
+          mbar_arrive_peer(peer_addr(&pfull[st], 0));
         }
-        mbar_arrive_peer(peer_addr(&pfull[st], 0));
       }
     } else if (lane == 0) {
       constexpr uint32_t idesc = idesc_u8(256, NQ);
@@ -766,8 +803,10 @@ __global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(TScanArgs a)
         tc_fence_after();
         for (uint32_t kc = 0; kc < KC; kc++, g++) {
           const uint32_t st = g % S_, n = g / S_;
-          if (!mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, false) ||
-              !mbar_wait_pair(&pfull[st], n & 1, a.wait_ns, abort_s, true)) {
+          const bool landed = TMA ? mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, true)
+                                  : mbar_wait_pair(&full[st], n & 1, a.wait_ns, abort_s, false) &&
+                                        mbar_wait_pair(&pfull[st], n & 1, a.wait_ns, abort_s, true);
+          if (!landed) {
             if (!*abort_s) pair_abort(abort_s, a.err);
             stop = true;
             break;
@@ -826,7 +865,17 @@ __global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(TScanArgs a)
     // copies issued but perhaps never consumed must land before the shared
     // memory is released (only after a wait gave up)
     const uint32_t iss = *issued_s;
-    for (uint32_t g = iss > S_ ? iss - S_ : 0; g < iss; g++) mbar_wait(&full[g % S_], (g / S_) & 1, a.wait_ns);
+    if (!TMA || rank == 0)
+      for (uint32_t g = iss > S_ ? iss - S_ : 0; g < iss; g++) mbar_wait(&full[g % S_], (g / S_) & 1, a.wait_ns);
+    if (TMA) {
+      // a tensor-map copy completes on the leader's barrier, which may never
+      // see its phase when the two CTAs stopped at different chunks: give the
+      // copies in flight a fixed 50 us (they take a few) before either CTA
+      // leaves
+      const uint64_t t0 = gtimer();
+      while (gtimer() - t0 < 50000) {
+      }
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -952,14 +1001,49 @@ int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
   return 0;
 }
 
-template <int NQ, int MTPC>
+// cuTensorMapEncodeTiled, from the driver through the runtime (no link
+// against the driver library); null when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// `rows` rows of 128 bytes at base, copied box_rows rows at a time, as they
+// lie (the data is stored pre-swizzled, so no swizzle mode).
+bool encode_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc || rows == 0 || rows > (1ull << 31) || box_rows == 0 || box_rows > 256 ||
+      (reinterpret_cast<uintptr_t>(base) & 15))
+    return false;
+  const cuuint64_t dims[2] = {128, rows};
+  const cuuint64_t strides[1] = {128};
+  const cuuint32_t box[2] = {128, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int NQ, int MTPC, bool TMA>
 int launch_t2(const TScanArgs& a0, int stages, cudaStream_t st) {
   TScanArgs a = a0;
   a.stages = (uint32_t)stages;
   constexpr uint32_t STAGE = MTPC * TBLK + NQ / 2 * 128;
   const size_t smem = 1024 + (size_t)stages * STAGE + (3 * stages + 5) * 8 + 16;
   if (smem > 227 * 1024 || a.mt_total % (2 * MTPC)) return -1;
-  set_smem(tscan2_kernel<NQ, MTPC>, smem);
+  CUtensorMap qmap;
+  memset(&qmap, 0, sizeof(qmap));
+  if (TMA && (!a.tmaps || !encode_rows(&qmap, a.qb, (uint64_t)4 * a.kc_total * a.nq_rows, NQ / 2))) return -1;
+  set_smem(tscan2_kernel<NQ, MTPC, TMA>, smem);
   const size_t items = (size_t)a.nshards * 4 * (a.mt_total / (2 * MTPC)) * a.groups;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -974,7 +1058,7 @@ int launch_t2(const TScanArgs& a0, int stages, cudaStream_t st) {
   cfg.numAttrs = 1;
   cfg.gridDim = dim3(2);
   int clusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&clusters, tscan2_kernel<NQ, MTPC>, &cfg) != cudaSuccess || clusters < 1) {
+  if (cudaOccupancyMaxActiveClusters(&clusters, tscan2_kernel<NQ, MTPC, TMA>, &cfg) != cudaSuccess || clusters < 1) {
     cudaGetLastError();
     return -1;
   }
@@ -984,7 +1068,7 @@ int launch_t2(const TScanArgs& a0, int stages, cudaStream_t st) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   clusters = std::min(clusters, sms / 2);
   cfg.gridDim = dim3((unsigned)(2 * std::min<size_t>(items, (size_t)clusters)));
-  return cudaLaunchKernelEx(&cfg, tscan2_kernel<NQ, MTPC>, a) == cudaSuccess ? 0 : -1;
+  return cudaLaunchKernelEx(&cfg, tscan2_kernel<NQ, MTPC, TMA>, a, qmap) == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace
@@ -1018,6 +1102,9 @@ const TScanShape* tscan_shapes(int* count) {
       // CTA pairs (tcgen05.mma.cta_group::2): rows are the pair's query
       // operand rows (each CTA stages half of them)
       {64, 1, 8, 2},  {128, 1, 6, 2}, {128, 2, 4, 2}, {256, 1, 6, 2}, {256, 2, 4, 2},
+      // CTA pairs loading with tensor maps: both CTAs' copies complete on the
+      // leader's barrier (no relay)
+      {64, 1, 8, 3},  {128, 1, 6, 3}, {128, 2, 4, 3}, {256, 1, 6, 3}, {256, 2, 4, 3},
   };
   *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
   return shapes;
@@ -1029,9 +1116,22 @@ size_t tscan_query_bytes(const Group& g, int nb_pad) {
   return (size_t)4 * kc * 4 * nb_pad * 128;
 }
 
+int tscan_slab_maps(uint8_t* const* host_slabs, int nshards, const Group& g, void* dev_maps) {
+  uint32_t mt, kc;
+  tensor_dims(g, &mt, &kc);
+  std::vector<CUtensorMap> maps((size_t)nshards);
+  for (int s = 0; s < nshards; s++)
+    if (!encode_rows(&maps[s], host_slabs[s], (uint64_t)4 * mt * kc * 128, 128)) return -1;
+  return cudaMemcpy(dev_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice) == cudaSuccess
+             ? 0
+             : -1;
+}
+
+size_t tscan_slab_map_bytes(int nshards) { return (size_t)nshards * sizeof(CUtensorMap); }
+
 int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, size_t q_stride, int nb, int nb_pad,
                  uint8_t* qb, uint32_t* out, uint32_t* err, const Group& g, const SlotMaps& maps,
-                 const TScanShape& shape, cudaStream_t st, const TScanLimits& lim) {
+                 const TScanShape& shape, cudaStream_t st, const TScanLimits& lim, const void* slab_maps) {
   uint32_t mt, kc;
   tensor_dims(g, &mt, &kc);
   const int qpc = shape.nq / 4;
@@ -1055,14 +1155,25 @@ int launch_tscan(uint8_t* const* slabs_dev, int nshards, const uint32_t* qnat, s
   a.stages = 0;
   a.wait_ns = lim.wait_ns ? lim.wait_ns : WAIT_NS;
   a.withhold = lim.withhold < 0 ? ~0u : (uint32_t)lim.withhold;
+  a.tmaps = static_cast<const CUtensorMap*>(slab_maps);
   const int stg = shape.stages;
   if (shape.persistent == 2) {
     switch (shape.nq * 10 + shape.mtpc) {
-      case 641: return launch_t2<64, 1>(a, stg, st);
-      case 1281: return launch_t2<128, 1>(a, stg, st);
-      case 1282: return launch_t2<128, 2>(a, stg, st);
-      case 2561: return launch_t2<256, 1>(a, stg, st);
-      case 2562: return launch_t2<256, 2>(a, stg, st);
+      case 641: return launch_t2<64, 1, false>(a, stg, st);
+      case 1281: return launch_t2<128, 1, false>(a, stg, st);
+      case 1282: return launch_t2<128, 2, false>(a, stg, st);
+      case 2561: return launch_t2<256, 1, false>(a, stg, st);
+      case 2562: return launch_t2<256, 2, false>(a, stg, st);
+      default: return -1;
+    }
+  }
+  if (shape.persistent == 3) {
+    switch (shape.nq * 10 + shape.mtpc) {
+      case 641: return launch_t2<64, 1, true>(a, stg, st);
+      case 1281: return launch_t2<128, 1, true>(a, stg, st);
+      case 1282: return launch_t2<128, 2, true>(a, stg, st);
+      case 2561: return launch_t2<256, 1, true>(a, stg, st);
+      case 2562: return launch_t2<256, 2, true>(a, stg, st);
       default: return -1;
     }
   }

@@ -216,7 +216,7 @@ def test_empty_call_and_largest_group(config1_pair):
         assert np.array_equal(orc.process_reply(r, seed), data[j % 2][i].astype(np.int64)), k
 
 
-@pytest.mark.parametrize("persistent", [0, 1, 2])
+@pytest.mark.parametrize("persistent", [0, 1, 2, 3])
 def test_scan_wait_runs_out_and_the_device_stays_usable(persistent):
     # the timeout path of the tensor scan's bounded waits: with a 2 ms limit
     # and the first block's producer withholding one chunk, that block's MMA
@@ -227,8 +227,10 @@ def test_scan_wait_runs_out_and_the_device_stays_usable(persistent):
     n = 256
     _, fa, fb = _pair(8, 256, 256, 1, 1, 77)
     if persistent:
-        # the persistent one-CTA kernel, or the CTA-pair kernel (whose leader
-        # then gives up and raises the pair's abort flag for its follower)
+        # the persistent one-CTA kernel, or a CTA-pair kernel (whose leader
+        # then gives up and raises the pair's abort flag for its follower;
+        # with tensor-map copies the follower's copies of the chunks its
+        # leader never armed land on the leader's barrier regardless)
         shapes = dp.tscan_shapes()
         fb.set_tile(1, next(i for i, s in enumerate(shapes) if s[3] == persistent))
     q = _qnat(torch, 1, n, 78)
