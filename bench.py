@@ -72,6 +72,9 @@ ENTRIES_DEFAULT = 1 << 22
 PAYLOAD = 2560
 REF_RESPONSE_S_8T = 4.3  # ARTIFACT-APPENDIX.md:122 (2^22 x 2560 B, 8 threads, Xeon Gold 5318S)
 METRIC = "pir_responses_per_sec_2p22"
+# the tensor scan kernel of a tile shape (its fourth field)
+TILE_KERNELS = ("tscan_kernel (one tile per CTA)", "tscanp_kernel (persistent)",
+                "tscan2_kernel (CTA pair, relayed bulk copies)", "tscan2_kernel (CTA pair, tensor-map copies)")
 UNIT = "responses/s"
 
 
@@ -609,7 +612,8 @@ def batched_leg(dp, torch, dev, entries, engine, sizes, groups, check_every=8):
         if engine == "tensor":
             ch, tms, shapes = fleet.tune(B, pipeline=True)
             tile = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
-                    "persistent": bool(shapes[ch][3]), "schedule": fleet.get_schedule(B)}
+                    "persistent": bool(shapes[ch][3]), "kernel": TILE_KERNELS[shapes[ch][3]],
+                    "schedule": fleet.get_schedule(B)}
         else:
             pb, _ = fleet.tune_cuda_cores(B)
             tile = {"queries_per_block": pb}
@@ -918,13 +922,14 @@ def main():
                     fleet.set_schedule(B, forced[B][1])
                 sh = dp.tscan_shapes()[forced[B][0]]
                 shape = {"rows_per_cta": sh[0], "mtiles_per_cta": sh[1], "stages": sh[2], "persistent": bool(sh[3]),
+                         "kernel": TILE_KERNELS[sh[3]],
                          "schedule": {"order": ("overlap", "serial", "last chunk")[fleet.get_schedule(B) & 3],
                                       "cluster_chains": bool(fleet.get_schedule(B) & 4)},
                          "tuner": "forced (--tile)"}
             elif args.engine == "tensor":
                 ch, tms, shapes = fleet.tune(B, pipeline=True)
                 shape = {"rows_per_cta": shapes[ch][0], "mtiles_per_cta": shapes[ch][1], "stages": shapes[ch][2],
-                         "persistent": bool(shapes[ch][3]),
+                         "persistent": bool(shapes[ch][3]), "kernel": TILE_KERNELS[shapes[ch][3]],
                          "schedule": {"order": ("overlap", "serial", "last chunk")[fleet.get_schedule(B) & 3],
                                       "cluster_chains": bool(fleet.get_schedule(B) & 4)},
                          "tuned_ms_per_group": round(float(tms[ch]), 3), "tuner": "whole-group pipeline"}
