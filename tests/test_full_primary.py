@@ -155,9 +155,9 @@ def test_engines_scan_words_agree_at_full_primary(shards, fleets_512):
 
 
 def test_cta_pair_tiles_at_full_primary(shards, fleets_512):
-    # every CTA-pair tile of the tensor scan (tcgen05.mma.cta_group::2) at
-    # K = 6144 with both signs: scan words equal the CUDA-core engine's for a
-    # group of 64 arbitrary query vectors
+    # every CTA-pair tile of the tensor scan (tcgen05.mma.cta_group::2), both
+    # load forms, at K = 6144 with both signs: scan words equal the CUDA-core
+    # engine's for a group of 64 arbitrary query vectors
     torch = pytest.importorskip("torch")
     gen = np.random.default_rng(17)
     nq = 64
@@ -177,7 +177,8 @@ def test_cta_pair_tiles_at_full_primary(shards, fleets_512):
 
     want = scan(fleets_512[dp.ENGINE_CUDA_CORES])
     ft = fleets_512[dp.ENGINE_TENSOR]
-    pairs = [i for i, s in enumerate(dp.tscan_shapes()) if s[3] == 2]
+    # relayed bulk copies (2) and tensor-map copies on the leader's barrier (3)
+    pairs = [i for i, s in enumerate(dp.tscan_shapes()) if s[3] in (2, 3)]
     assert pairs
     try:
         for i in pairs:
