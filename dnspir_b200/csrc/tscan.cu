@@ -114,6 +114,24 @@ __device__ __forceinline__ void tma_load_pair(void* dst, const CUtensorMap* map,
       : "memory");
 }
 
+// The same with an L2 cache policy (createpolicy): the query operand, which
+// every CTA re-reads for every slab tile, is kept in L2 with evict_last --
+// without it the tensor-map copies of the query operand went back to DRAM
+// (at 256 queries the pair kernel read 2.9 x the slab bytes from DRAM).
+__device__ __forceinline__ void tma_load_pair_hint(void* dst, const CUtensorMap* map, int x, int y, uint32_t mbar,
+                                                   uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
+      "[%1, {%2, %3}], [%4], %5;" ::"r"(sa(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(mbar), "l"(policy)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -734,6 +752,7 @@ __global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(const __grid
     if (lane == 0) {
       uint32_t g = 0;
       bool stop = false;
+      const uint64_t vpol = TMA ? l2_evict_last_policy() : 0;
       for (uint32_t item = cid; item < items && !stop; item += ncl) {
         uint32_t grp, mt0, sgn;
         int p, s;
@@ -762,8 +781,8 @@ __global__ void __launch_bounds__(tscanp_nt<NQ>(), 1) tscan2_kernel(const __grid
             const int arow = (int)(((ps * a.mt_total + mt0 + rank * MTPC) * KC + kc) * 128);
 #pragma unroll
             for (int t = 0; t < MTPC; t++) tma_load_pair(dst + t * TBLK, a.tmaps + s, 0, arow + t * (int)KC * 128, fb);
-            tma_load_pair(dst + A_BYTES, &qmap, 0,
-                          (int)((ps * KC + kc) * a.nq_rows + (size_t)grp * NQ + rank * (NQ / 2)), fb);
+            tma_load_pair_hint(dst + A_BYTES, &qmap, 0,
+                               (int)((ps * KC + kc) * a.nq_rows + (size_t)grp * NQ + rank * (NQ / 2)), fb, vpol);
           } else {
             mbar_expect_tx(&full[st], STAGE);
 #pragma unroll
@@ -996,7 +1015,10 @@ int launch_tp(const TScanArgs& a0, int stages, cudaStream_t st) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const size_t items = (size_t)a.nshards * 4 * (a.mt_total / MTPC) * a.groups;
-  const size_t grid = std::min(items, (size_t)sms * per_sm);
+  size_t grid = std::min(items, (size_t)sms * per_sm);
+  // a multiple of the query-group count, so that the CTAs sharing a slab
+  // tile are the same in every round (as for the CTA pairs below)
+  if (grid >= a.groups) grid -= grid % a.groups;
   tscanp_kernel<NQ, MTPC><<<(unsigned)grid, tscanp_nt<NQ>(), smem, st>>>(a);
   return 0;
 }
@@ -1067,6 +1089,12 @@ int launch_t2(const TScanArgs& a0, int stages, cudaStream_t st) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   clusters = std::min(clusters, sms / 2);
+  // the query groups of one slab tile are consecutive items: with a cluster
+  // count that is a multiple of the group count, the same clusters share a
+  // slab tile in every round and stay in step, so the tile comes from HBM
+  // once and from L2 for the other groups (74 clusters at 4 groups drifted
+  // apart and read the slabs three times over)
+  if (clusters >= (int)a.groups) clusters -= clusters % (int)a.groups;
   cfg.gridDim = dim3((unsigned)(2 * std::min<size_t>(items, (size_t)clusters)));
   return cudaLaunchKernelEx(&cfg, tscan2_kernel<NQ, MTPC, TMA>, a, qmap) == cudaSuccess ? 0 : -1;
 }
