@@ -1133,6 +1133,10 @@ const TScanShape* tscan_shapes(int* count) {
       // CTA pairs loading with tensor maps: both CTAs' copies complete on the
       // leader's barrier (no relay)
       {64, 1, 8, 3},  {128, 1, 6, 3}, {128, 2, 4, 3}, {256, 1, 6, 3}, {256, 2, 4, 3},
+      // a deeper persistent ring for 16-query groups, whose scan is HBM-bound
+      // (30.1 ms per group at 2^22 against 29.5-30.9 for the one-tile-per-CTA
+      // shapes; (64, 1, 8-9) and (128, 1, 6-7) measured 35-37 ms)
+      {64, 2, 5, 1},
   };
   *count = (int)(sizeof(shapes) / sizeof(shapes[0]));
   return shapes;
