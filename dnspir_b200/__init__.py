@@ -298,7 +298,9 @@ ENGINE_TENSOR = 1
 
 def tscan_shapes():
     """The tensor scan's tile shapes: (query-operand rows, m-tiles, stages,
-    persistent) per CTA."""
+    kernel) per CTA; kernel 0 is one tile per CTA, 1 the persistent
+    warp-specialised kernel, 2 and 3 the CTA pair (relayed bulk copies,
+    tensor-map copies)."""
     n = lib().dnspir_tscan_shapes(None, None, None, None, 0)
     a = [np.zeros(n, dtype=np.int32) for _ in range(4)]
     lib().dnspir_tscan_shapes(*[_ptr(x) for x in a], n)

@@ -202,8 +202,9 @@ int dnspir_fleet_set_tile(dnspir_fleet* fleet, uint32_t batch, int shape_index);
  * the reference. */
 int dnspir_fleet_set_wait_limit(dnspir_fleet* fleet, uint64_t wait_ns, int withhold_chunk);
 /* The tensor scan's tile shapes (query-operand rows per CTA, m-tiles per CTA,
- * pipeline stages, 1 for the persistent warp-specialised kernel); returns
- * their count. */
+ * pipeline stages, kernel: 0 one tile per CTA, 1 persistent warp-specialised,
+ * 2 CTA pair with relayed bulk copies, 3 CTA pair with tensor-map copies);
+ * returns their count. */
 int dnspir_tscan_shapes(int* nq, int* mtpc, int* stages, int* persistent, int max);
 
 /* ---- Serving loop (no counterpart in the reference, whose server answers each
