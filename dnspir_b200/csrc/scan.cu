@@ -241,7 +241,7 @@ __device__ __forceinline__ uint32_t ms_encode12(uint64_t v) {
   return (uint32_t)r & ((1u << PRIM_B_BITS) - 1);
 }
 
-__global__ void __launch_bounds__(EPI_NT) primary_epilogue2k_kernel(
+__global__ void __launch_bounds__(EPI_NT, 3) primary_epilogue2k_kernel(
     const uint32_t* __restrict__ fin, int nshards, const uint32_t* __restrict__ a_ms,
     const int* __restrict__ distinct_of, uint16_t* __restrict__ sec_in, int nq, int chunk,
     const uint32_t* __restrict__ uof, NttTables T, uint32_t k1, uint32_t k1q, uint32_t k2, uint32_t k2q) {
