@@ -324,6 +324,12 @@ int dnspir_fleet_create_general(int device, uint32_t log2_n, uint32_t primary_or
     CK(cudaEventCreateWithFlags(&s.sec_done, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&s.sec_tail, cudaEventDisableTiming));
   }
+  {
+    // timing events of the first 64 groups of a call, made now rather than
+    // between the launches of a call's first long run of groups
+    cudaEvent_t* unused = nullptr;
+    CKR(group_events(f.get(), 63, &unused));
+  }
   f->slabs.assign(num_distinct, nullptr);
   f->ready.assign(num_distinct, false);
   const size_t words = slab_words(f->g1);
